@@ -1,0 +1,259 @@
+/*
+ * mordred_b200.h — C ABI of the B200 (sm_100a) star-query hot path.
+ *
+ * Every entry point takes plain device pointers and sizes, is stream-ordered and
+ * asynchronous on the stream it is given (NULL = legacy default stream), never
+ * allocates on the query path and returns an int status (MB_OK = 0). Kernels report
+ * data errors (a key outside its hash table, a group index outside the result array,
+ * a pipeline wait that ran out) through a per-device status word that
+ * mb_device_status() reads; they never trap.
+ *
+ * Ownership follows the reference: the caller allocates and zeroes every hash table
+ * and result buffer (src/gpudb/QueryOptimizer.cu:2726-2748,3554-3571,
+ * src/ssb/q21.cu:151-166); kernels accumulate into what they are given, so several
+ * calls (segment groups, CPU + GPU halves) can add into one result.
+ *
+ * Each entry point names the reference interface it replaces (file:line within the
+ * reference project).
+ */
+#ifndef MORDRED_B200_H
+#define MORDRED_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A cudaStream_t passed as an opaque pointer (NULL = legacy default stream). */
+typedef void* mb_stream_t;
+
+/* ---- status codes ------------------------------------------------------------ */
+#define MB_OK 0
+#define MB_ERR_ARG 1         /* bad argument (NULL where required, bad enum, bad size) */
+#define MB_ERR_ALIGN 2       /* a column or table pointer breaks the required alignment */
+#define MB_ERR_LAUNCH 3      /* kernel launch failed */
+#define MB_ERR_CUDA 4        /* a CUDA runtime call failed */
+#define MB_ERR_NODEV 5       /* no CUDA device / device init failed */
+#define MB_ERR_SIZE 6        /* size beyond a documented maximum */
+
+/* ---- device status bits (sticky until cleared by mb_device_status) ----------- */
+#define MB_STATUS_PROBE_RANGE 0x1u  /* (key - key_min) % num_slots < 0: row treated as a miss */
+#define MB_STATUS_GROUP_RANGE 0x2u  /* group index outside [0, total_val): row skipped */
+#define MB_STATUS_TIMEOUT 0x4u      /* a bounded pipeline wait ran out; result incomplete */
+
+/* ---- enums ---------------------------------------------------------------------- */
+/* Filter modes: KernelArgs.h:44-86 (pred_eq, pred_between, pred_eq_or_eq),
+ * build mode numbering GPUProcessing.h:971-982 (0 = EQ, 1 = BETWEEN, 2 = EQ OR EQ). */
+#define MB_FILTER_EQ 0
+#define MB_FILTER_BETWEEN 1
+#define MB_FILTER_EQ_OR_EQ 2
+
+/* Hash-table layouts. slot = (key - key_min) % num_slots (crystal/join.cuh:3).
+ *  MB_HT_KEY      int ht[num_slots]; ht[slot] = key; nonzero = present; no payload
+ *                 (BlockBuildSelectivePHT_1 / BlockProbeAndPHT_1, crystal/join.cuh:5-82,167-234)
+ *  MB_HT_KEY_VAL  int ht[2*num_slots]; {key, val}; the 8-byte slot nonzero = present;
+ *                 payload = upper 32 bits = val (crystal/join.cuh:84-165,236-311)
+ *  MB_HT_VAL_OFF  int ht[2*num_slots]; {val, row+1}; the 8-byte slot nonzero = present;
+ *                 payload = lower 32 bits = val (engine layout, BlockLibrary.cuh:86-111,594-735) */
+#define MB_HT_KEY 0
+#define MB_HT_KEY_VAL 1
+#define MB_HT_VAL_OFF 2
+
+/* Aggregates (int32 arithmetic, then widened to 64 bits, as q11.cu:74, q41.cu:76). */
+#define MB_AGG_SUM 0   /* a0           */
+#define MB_AGG_SUB 1   /* a0 - a1      (KernelArgs.h:20-24, group-by kernels) */
+#define MB_AGG_MUL 2   /* a0 * a1      (KernelArgs.h:26-30, aggregate kernels) */
+#define MB_AGG_MUL_PAYLOAD 3 /* a0 * payload of probe 0 (src/ops/join.cu:73) */
+
+/* Result layouts. */
+#define MB_RES_SCALAR 0   /* unsigned long long res[1] */
+#define MB_RES_ENGINE6 1  /* int res[6*total_val]: g1..g4 at [6h..6h+3], u64 sum at [6h+4] (GPUProcessing.h:143-150) */
+#define MB_RES_CRYSTAL4 2 /* int res[4*total_val]: two keys at [4h],[4h+1], u64 sum at [4h+2] (q21.cu:65-68) */
+#define MB_RES_DENSE 3    /* unsigned long long res[total_val] (sums only) */
+
+#define MB_MAX_FILTERS 3
+#define MB_MAX_PROBES 4
+
+/* ---- generic fused star query ------------------------------------------------- */
+typedef struct mb_filter {
+  const int* col;  /* fact column (or per-segment cache-slot index array in segment mode) */
+  int mode;        /* MB_FILTER_* */
+  int c1, c2;      /* EQ: x == c1; BETWEEN: c1 <= x <= c2; EQ_OR_EQ: x == c1 || x == c2 */
+} mb_filter;
+
+typedef struct mb_probe {
+  const int* fkey;          /* fact foreign-key column (or cache-slot index array) */
+  const int* ht;            /* hash table in `layout` */
+  int num_slots;            /* ht_len */
+  int key_min;              /* keys_min */
+  int layout;               /* MB_HT_* */
+  int min_val;              /* group term (payload - min_val) * unique_val */
+  int unique_val;
+  int res_slot;             /* ENGINE6: key column 0..3; CRYSTAL4: 0 or 1; -1: payload not stored */
+  const uint32_t* presence; /* optional presence bitmap built by mb_build_* (bit s = slot s present) */
+} mb_probe;
+
+typedef struct mb_star_args {
+  int64_t num_rows;
+  int num_filters;
+  mb_filter filter[MB_MAX_FILTERS];
+  int num_probes;           /* probes run in array order */
+  mb_probe probe[MB_MAX_PROBES];
+  const int* aggr[2];       /* aggregate columns (aggr[1] NULL for MB_AGG_SUM) */
+  int agg_op;               /* MB_AGG_* */
+  int total_val;            /* number of groups (1 for MB_RES_SCALAR) */
+  int group_bias;           /* constant added to the group sum before % total_val */
+  int res_layout;           /* MB_RES_* */
+  void* res;                /* device result, zeroed by the caller; accumulated into */
+  unsigned long long* count;/* optional: rows passing the first count_after filters (u64, accumulated) */
+  int count_after;          /* -1 = rows passing every filter and probe */
+  /* Segment-cache addressing (src/gpudb/GPUProcessing.h:54-67). When gpu_cache is
+   * non-NULL every column field above holds a per-segment cache-slot index array and
+   * row r of the call reads gpu_cache[slot(seg(r)) * segment_size + r % segment_size]. */
+  const int* gpu_cache;
+  const short* segment_group; /* virtual segment -> segment id; NULL: (start_offset + r) / segment_size */
+  int64_t start_offset;
+  int segment_size;           /* power of two (reference: 1,048,576) */
+  /* launch configuration; 0 = the tuned default for this shape */
+  int threads;                /* 128, 256 or 512 */
+  int items_per_thread;       /* 4, 8 or 16 */
+  int stages;                 /* 2..8 bulk-copy stages */
+  int grid;                   /* CTAs; 0 = one wave of resident CTAs */
+} mb_star_args;
+
+/* Fused filter -> chained probe -> group-by/aggregate over the fact table.
+ * Generalises filter_probe_group_by_GPU2 / probe_group_by_GPU2 / filter_probe_aggr_GPU2 /
+ * probe_aggr_GPU2 (src/gpudb/GPUProcessing.h:17-155,275-391,1526-1776) and the SSB
+ * probe kernels (src/ssb/q11.cu:25-93, q21.cu:25-72, q41.cu:25-80). */
+int mb_star_query(const mb_star_args* args, mb_stream_t stream);
+
+/* ---- Crystal-level builds and the src/ops operators ----------------------------- */
+/* Filtered perfect-hash build. filter_col NULL = no filter. dim_val NULL builds the
+ * MB_HT_KEY layout (BlockBuildSelectivePHT_1), else MB_HT_KEY_VAL (…_PHT_2).
+ * presence (optional, zeroed by the caller, (num_slots+31)/32 words) receives the slot bitmap.
+ * Replaces build_hashtable_s/p/c/d (src/ssb/q21.cu:74-138, src/ssb/q41.cu:82-167). */
+int mb_build_pht(const int* filter_col, int filter_mode, int c1, int c2,
+                 const int* dim_key, const int* dim_val, int num_tuples,
+                 int* ht, int num_slots, int key_min, uint32_t* presence,
+                 mb_stream_t stream);
+
+/* Unfiltered PHT_2 build: src/ops/join.cu:21-40 build_kernel. */
+int mb_join_build(const int* dim_key, const int* dim_val, int num_tuples,
+                  int* hash_table, int num_slots, mb_stream_t stream);
+
+/* Probe and sum fact_val * dim_val: src/ops/join.cu:42-85 probe_kernel. */
+int mb_join_probe(const int* fact_fkey, const int* fact_val, int num_tuples,
+                  const int* hash_table, int num_slots, unsigned long long* res,
+                  mb_stream_t stream);
+
+/* ---- SSB query kernels with the reference signatures ---------------------------- */
+/* src/ssb/q11.cu:25-93 QueryKernel: revenue += sum(extendedprice*discount) over
+ * 1<=discount<=3, quantity<25, 19930000<orderdate<19940000; d_total (optional) +=
+ * rows passing the discount and quantity predicates. */
+int mb_q11_query(const int* lo_orderdate, const int* lo_discount, const int* lo_quantity,
+                 const int* lo_extendedprice, int lo_num_entries,
+                 unsigned long long* revenue, int* d_total, mb_stream_t stream);
+
+/* src/ssb/q21.cu:25-72 probe: res int[4*7000], group (brand*7 + year-1992) % 7000. */
+int mb_q21_probe(const int* lo_orderdate, const int* lo_partkey, const int* lo_suppkey,
+                 const int* lo_revenue, int lo_len,
+                 const int* ht_s, int s_len, const int* ht_p, int p_len,
+                 const int* ht_d, int d_len, int* res, mb_stream_t stream);
+
+/* src/ssb/q41.cu:25-80 probe: res int[4*175], group (c_nation*7 + year-1992) % 175. */
+int mb_q41_probe(const int* lo_orderdate, const int* lo_partkey, const int* lo_custkey,
+                 const int* lo_suppkey, const int* lo_revenue, const int* lo_supplycost,
+                 int lo_len, const int* ht_p, int p_len, const int* ht_s, int s_len,
+                 const int* ht_c, int c_len, const int* ht_d, int d_len, int* res,
+                 mb_stream_t stream);
+
+/* ---- engine (src/gpudb) kernel arguments, restated as plain C ------------------- */
+/* KernelArgs.h:270-286 filterArgsGPU; device predicate function pointers become mode1/mode2. */
+typedef struct mb_filterArgsGPU {
+  const int* filter_idx1;
+  const int* filter_idx2;
+  int compare1, compare2, compare3, compare4;
+  int mode1, mode2;
+} mb_filterArgsGPU;
+
+/* KernelArgs.h:146-169 probeArgsGPU (slot 1..4 = supplier, customer, part, date). */
+typedef struct mb_probeArgsGPU {
+  const int* key_idx1; const int* key_idx2; const int* key_idx3; const int* key_idx4;
+  const int* ht1; const int* ht2; const int* ht3; const int* ht4;
+  int dim_len1, dim_len2, dim_len3, dim_len4;
+  int min_key1, min_key2, min_key3, min_key4;
+} mb_probeArgsGPU;
+
+/* KernelArgs.h:218-242 groupbyArgsGPU; the device group function pointer becomes mode
+ * (0 = aggr1 - aggr2, 1 = aggr1 * aggr2). */
+typedef struct mb_groupbyArgsGPU {
+  const int* aggr_idx1; const int* aggr_idx2;
+  const int* group_idx1; const int* group_idx2; const int* group_idx3; const int* group_idx4;
+  int min_val1, min_val2, min_val3, min_val4;
+  int unique_val1, unique_val2, unique_val3, unique_val4;
+  int total_val;
+  int mode;
+} mb_groupbyArgsGPU;
+
+/* KernelArgs.h:196-205 buildArgsGPU. */
+typedef struct mb_buildArgsGPU {
+  const int* key_idx;
+  const int* val_idx;
+  int num_slots;
+  int val_min;
+  int val_max;
+} mb_buildArgsGPU;
+
+/* GPUProcessing.h:17-155 filter_probe_group_by_GPU2, launched by
+ * CPUGPUProcessing.cu:221-354 call_pfilter_probe_group_by_GPU. res = int[6*total_val]. */
+int mb_filter_probe_group_by_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs,
+                                  const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs,
+                                  int num_tuples, int* res, int start_offset,
+                                  const short* segment_group, mb_stream_t stream);
+
+/* GPUProcessing.h:275-391 probe_group_by_GPU2 (CPUGPUProcessing.cu:802-916). */
+int mb_probe_group_by_GPU2(const int* gpuCache, const mb_probeArgsGPU* pargs,
+                           const mb_groupbyArgsGPU* gargs, int num_tuples, int* res,
+                           int start_offset, const short* segment_group, mb_stream_t stream);
+
+/* GPUProcessing.h:1675-1776 filter_probe_aggr_GPU2: u64 sum of aggr1*aggr2 at res[4]. */
+int mb_filter_probe_aggr_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs,
+                              const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs,
+                              int num_tuples, int* res, int start_offset,
+                              const short* segment_group, mb_stream_t stream);
+
+/* GPUProcessing.h:927-997 build_GPU2: engine layout {val, row+1}. */
+int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs,
+                  const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table,
+                  int start_offset, const short* segment_group, mb_stream_t stream);
+
+/* ---- synthetic data (seeded; identical on host and device) ---------------------- */
+/* Fact column `col` (MB_LO_* in mordred_b200/csrc/ssbgen.h) rows [row0, row0+n) into a
+ * device buffer. s_len/c_len/p_len give the foreign-key ranges. */
+int mb_gen_fact_column(int col, uint64_t seed, int64_t row0, int64_t n,
+                       int s_len, int c_len, int p_len, int* out, mb_stream_t stream);
+/* Dimension column (MB_D_*, MB_S_*, MB_C_*, MB_P_*) rows [0, n) into a device buffer. */
+int mb_gen_dim_column(int col, uint64_t seed, int64_t n, int* out, mb_stream_t stream);
+/* Host versions (nthreads <= 0: all hardware threads). */
+int mb_gen_fact_column_host(int col, uint64_t seed, int64_t row0, int64_t n,
+                            int s_len, int c_len, int p_len, int* out, int nthreads);
+int mb_gen_dim_column_host(int col, uint64_t seed, int64_t n, int* out, int nthreads);
+
+/* ---- runtime ---------------------------------------------------------------------- */
+int mb_version(void);
+/* Per-device set-up (kernel attributes, the device status word). Called implicitly by
+ * the first launch on a device; call it explicitly before capturing a CUDA graph. */
+int mb_init(int device);
+/* Read (and optionally clear) the device status bits; synchronises the device. */
+int mb_device_status(int device, unsigned int* status, int clear);
+const char* mb_error_string(int code);
+/* Number of kernel launches issued by this library in this process (all devices). */
+unsigned long long mb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MORDRED_B200_H */

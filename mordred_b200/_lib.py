@@ -1,0 +1,169 @@
+"""ctypes binding of the C ABI in ``include/mordred_b200.h``.
+
+The library is the in-tree ``libmordred_b200.so`` built by :mod:`mordred_b200.build`.
+Loading never falls back to anything else: if the library is missing or does not
+load, :func:`lib` raises, so no query can silently run off the GPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from . import build as _build
+
+# ---- constants (mirror include/mordred_b200.h) -------------------------------------
+MB_OK = 0
+MB_STATUS_PROBE_RANGE = 0x1
+MB_STATUS_GROUP_RANGE = 0x2
+MB_STATUS_TIMEOUT = 0x4
+
+MB_FILTER_EQ, MB_FILTER_BETWEEN, MB_FILTER_EQ_OR_EQ = 0, 1, 2
+MB_HT_KEY, MB_HT_KEY_VAL, MB_HT_VAL_OFF = 0, 1, 2
+MB_AGG_SUM, MB_AGG_SUB, MB_AGG_MUL, MB_AGG_MUL_PAYLOAD = 0, 1, 2, 3
+MB_RES_SCALAR, MB_RES_ENGINE6, MB_RES_CRYSTAL4, MB_RES_DENSE = 0, 1, 2, 3
+MB_MAX_FILTERS, MB_MAX_PROBES = 3, 4
+
+# generator column ids (mordred_b200/csrc/ssbgen.h)
+MB_LO_ORDERDATE, MB_LO_QUANTITY, MB_LO_DISCOUNT, MB_LO_EXTENDEDPRICE = 0, 1, 2, 3
+MB_LO_SUPPKEY, MB_LO_CUSTKEY, MB_LO_PARTKEY, MB_LO_REVENUE, MB_LO_SUPPLYCOST = 4, 5, 6, 7, 8
+MB_D_DATEKEY, MB_D_YEAR, MB_D_YEARMONTHNUM = 16, 17, 18
+MB_S_SUPPKEY, MB_S_CITY, MB_S_NATION, MB_S_REGION = 32, 33, 34, 35
+MB_C_CUSTKEY, MB_C_CITY, MB_C_NATION, MB_C_REGION = 48, 49, 50, 51
+MB_P_PARTKEY, MB_P_BRAND1, MB_P_CATEGORY, MB_P_MFGR = 64, 65, 66, 67
+
+
+class MbFilter(C.Structure):
+    _fields_ = [("col", C.c_void_p), ("mode", C.c_int), ("c1", C.c_int), ("c2", C.c_int)]
+
+
+class MbProbe(C.Structure):
+    _fields_ = [("fkey", C.c_void_p), ("ht", C.c_void_p), ("num_slots", C.c_int),
+                ("key_min", C.c_int), ("layout", C.c_int), ("min_val", C.c_int),
+                ("unique_val", C.c_int), ("res_slot", C.c_int), ("presence", C.c_void_p)]
+
+
+class MbStarArgs(C.Structure):
+    _fields_ = [("num_rows", C.c_int64), ("num_filters", C.c_int),
+                ("filter", MbFilter * MB_MAX_FILTERS), ("num_probes", C.c_int),
+                ("probe", MbProbe * MB_MAX_PROBES), ("aggr", C.c_void_p * 2),
+                ("agg_op", C.c_int), ("total_val", C.c_int), ("group_bias", C.c_int),
+                ("res_layout", C.c_int), ("res", C.c_void_p), ("count", C.c_void_p),
+                ("count_after", C.c_int), ("gpu_cache", C.c_void_p),
+                ("segment_group", C.c_void_p), ("start_offset", C.c_int64),
+                ("segment_size", C.c_int), ("threads", C.c_int),
+                ("items_per_thread", C.c_int), ("stages", C.c_int), ("grid", C.c_int)]
+
+
+class MbFilterArgsGPU(C.Structure):
+    _fields_ = [("filter_idx1", C.c_void_p), ("filter_idx2", C.c_void_p),
+                ("compare1", C.c_int), ("compare2", C.c_int), ("compare3", C.c_int),
+                ("compare4", C.c_int), ("mode1", C.c_int), ("mode2", C.c_int)]
+
+
+class MbProbeArgsGPU(C.Structure):
+    _fields_ = ([(f"key_idx{i}", C.c_void_p) for i in range(1, 5)]
+                + [(f"ht{i}", C.c_void_p) for i in range(1, 5)]
+                + [(f"dim_len{i}", C.c_int) for i in range(1, 5)]
+                + [(f"min_key{i}", C.c_int) for i in range(1, 5)])
+
+
+class MbGroupbyArgsGPU(C.Structure):
+    _fields_ = ([("aggr_idx1", C.c_void_p), ("aggr_idx2", C.c_void_p)]
+                + [(f"group_idx{i}", C.c_void_p) for i in range(1, 5)]
+                + [(f"min_val{i}", C.c_int) for i in range(1, 5)]
+                + [(f"unique_val{i}", C.c_int) for i in range(1, 5)]
+                + [("total_val", C.c_int), ("mode", C.c_int)])
+
+
+class MbBuildArgsGPU(C.Structure):
+    _fields_ = [("key_idx", C.c_void_p), ("val_idx", C.c_void_p), ("num_slots", C.c_int),
+                ("val_min", C.c_int), ("val_max", C.c_int)]
+
+
+P = C.c_void_p
+I = C.c_int
+I64 = C.c_int64
+U64 = C.c_uint64
+PS = C.POINTER
+
+# name -> (restype, argtypes); every symbol declared in include/mordred_b200.h
+SIGNATURES = {
+    "mb_star_query": (I, [PS(MbStarArgs), P]),
+    "mb_build_pht": (I, [P, I, I, I, P, P, I, P, I, I, P, P]),
+    "mb_join_build": (I, [P, P, I, P, I, P]),
+    "mb_join_probe": (I, [P, P, I, P, I, P, P]),
+    "mb_q11_query": (I, [P, P, P, P, I, P, P, P]),
+    "mb_q21_probe": (I, [P, P, P, P, I, P, I, P, I, P, I, P, P]),
+    "mb_q41_probe": (I, [P, P, P, P, P, P, I, P, I, P, I, P, I, P, I, P, P]),
+    "mb_filter_probe_group_by_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbProbeArgsGPU),
+                                          PS(MbGroupbyArgsGPU), I, P, I, P, P]),
+    "mb_probe_group_by_GPU2": (I, [P, PS(MbProbeArgsGPU), PS(MbGroupbyArgsGPU), I, P, I, P, P]),
+    "mb_filter_probe_aggr_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbProbeArgsGPU),
+                                      PS(MbGroupbyArgsGPU), I, P, I, P, P]),
+    "mb_build_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbBuildArgsGPU), I, P, I, P, P]),
+    "mb_gen_fact_column": (I, [I, U64, I64, I64, I, I, I, P, P]),
+    "mb_gen_dim_column": (I, [I, U64, I64, P, P]),
+    "mb_gen_fact_column_host": (I, [I, U64, I64, I64, I, I, I, P, I]),
+    "mb_gen_dim_column_host": (I, [I, U64, I64, P, I]),
+    "mb_version": (I, []),
+    "mb_init": (I, [I]),
+    "mb_device_status": (I, [I, PS(C.c_uint), I]),
+    "mb_error_string": (C.c_char_p, [I]),
+    "mb_launch_count": (C.c_ulonglong, []),
+}
+
+
+class MbError(RuntimeError):
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed: {msg} (code {code})")
+        self.code = code
+
+
+_lock = threading.Lock()
+_lib: C.CDLL | None = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def lib() -> C.CDLL:
+    """Load (building first if the sources are newer) and return the library."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            path = lib_path()
+            if not os.path.exists(path) or not _build.up_to_date():
+                try:
+                    _build.build()
+                except Exception as e:  # nvcc missing on a box that only has the .so
+                    if not os.path.exists(path):
+                        raise ImportError(f"libmordred_b200.so is not built and cannot be built: {e}")
+            l = C.CDLL(path)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(l, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = l
+        return _lib
+
+
+def check(name: str, code: int) -> None:
+    if code != MB_OK:
+        msg = lib().mb_error_string(code).decode()
+        raise MbError(name, code, msg)
+
+
+def call(name: str, *args) -> None:
+    check(name, getattr(lib(), name)(*args))
+
+
+def device_status(device: int = -1, clear: bool = True) -> int:
+    st = C.c_uint(0)
+    call("mb_device_status", device, C.byref(st), 1 if clear else 0)
+    return st.value
+
+
+def launch_count() -> int:
+    return int(lib().mb_launch_count())

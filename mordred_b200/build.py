@@ -1,0 +1,70 @@
+"""Build the in-tree CUDA library ``mordred_b200/libmordred_b200.so`` for sm_100a.
+
+The library holds every kernel and the C ABI declared in ``include/mordred_b200.h``.
+It is compiled with nvcc directly (no JIT cache), so the built file travels with the
+source tree. Run ``python -m mordred_b200.build`` or call :func:`build`.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libmordred_b200.so")
+
+SOURCES = ["capi.cu", "star.cu", "build.cu"]
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    return "nvcc"
+
+
+def _sources() -> list[str]:
+    return [os.path.join(CSRC, s) for s in SOURCES]
+
+
+def _deps() -> list[str]:
+    out = []
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for base, _, files in os.walk(d):
+            out += [os.path.join(base, f) for f in files if f.endswith((".cu", ".cuh", ".h"))]
+    return out
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(p) <= t for p in _deps())
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    """Compile the library if any source is newer than it; return its path."""
+    if not force and up_to_date():
+        return LIB
+    cmd = [nvcc(), *GENCODE, "-lineinfo", "-O3", "-std=c++17", "--shared",
+           "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-I", os.path.join(ROOT, "include"),
+           "-o", LIB + ".tmp", *_sources(), "-lpthread"]
+    if ptxas_verbose:
+        cmd[1:1] = ["-Xptxas", "-v"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
+    if ptxas_verbose:
+        print(res.stderr, file=sys.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="-v" in sys.argv)
+    print(LIB)

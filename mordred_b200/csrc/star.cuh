@@ -1,0 +1,63 @@
+// star.cuh — the fused star-query pipeline: its device-side plan and the host launcher.
+//
+// One persistent kernel runs filter -> chained perfect-hash probes -> group-by /
+// aggregate over the fact table. Fact-column tiles stream into shared memory through
+// 1-D bulk copies (cp.async.bulk, no multicast) in a ring of mbarrier-tracked stages;
+// threads read them back with 128-bit shared loads, keep the selection of their rows
+// as a bitmask, probe L2-resident hash tables (or presence bitmaps staged in shared
+// memory) and accumulate 64-bit sums in registers (scalar) or in a shared-memory group
+// array that is flushed with one 64-bit atomic per touched group per CTA.
+#pragma once
+
+#include "common.cuh"
+
+namespace mb {
+
+constexpr int kMaxCols = MB_MAX_FILTERS + MB_MAX_PROBES + 2;
+constexpr int kMaxStages = 8;
+constexpr int kSmemGroupMax = 8192;            // groups kept in shared memory per CTA
+constexpr int kBitmapSmemMaxBytes = 32768;     // largest presence bitmap staged (262,144 slots)
+constexpr int kBitmapSmemTotalBytes = 40960;
+
+enum GroupMode { kGroupScalar = 0, kGroupSmem = 1, kGroupGlobal = 2 };
+
+struct StarPlan {
+  long long n;       // rows in this call
+  long long nfull;   // full tiles (the remainder runs with plain loads)
+  int ncols;
+  const int* col[kMaxCols];
+  int nf;
+  int f_col[MB_MAX_FILTERS], f_mode[MB_MAX_FILTERS], f_c1[MB_MAX_FILTERS], f_c2[MB_MAX_FILTERS];
+  int np;
+  int p_col[MB_MAX_PROBES];
+  const int* p_ht[MB_MAX_PROBES];
+  int p_slots[MB_MAX_PROBES], p_kmin[MB_MAX_PROBES], p_layout[MB_MAX_PROBES];
+  int p_min[MB_MAX_PROBES], p_mul[MB_MAX_PROBES], p_res_slot[MB_MAX_PROBES];
+  const uint32_t* p_presence[MB_MAX_PROBES];
+  int p_bm_off[MB_MAX_PROBES];    // byte offset of a staged bitmap in shared memory, -1 = none
+  int p_bm_words[MB_MAX_PROBES];
+  int a_col[2];
+  int agg_op;
+  int total_val, group_bias, res_layout;
+  void* res;
+  void* count;
+  int count32;                    // count is an int* (q11's d_total) rather than u64*
+  int count_after;
+  int gmode;
+  const int* gpu_cache;
+  const short* seg_group;
+  long long start_offset;
+  int seg_shift;
+  unsigned int* status;
+  int stages;
+  int smem_groups_off, smem_stage_off, stage_bytes, smem_total;
+};
+
+// Host: validate `a`, fill `plan`, pick the kernel variant and launch it on `stream`.
+// count32 makes `count` an int* accumulator.
+int launch_star(const mb_star_args* a, cudaStream_t stream, int count32);
+
+// Host: set per-device kernel attributes (dynamic shared memory opt-in).
+int star_init_device(const DeviceState& ds);
+
+}  // namespace mb
