@@ -117,10 +117,11 @@ typedef struct mb_star_args {
   int64_t start_offset;
   int segment_size;           /* power of two (reference: 1,048,576) */
   /* launch configuration; 0 = the tuned default for this shape */
-  int threads;                /* 128, 256 or 512 */
-  int items_per_thread;       /* 4, 8 or 16 */
+  int threads;                /* consumer threads per CTA: 128, 256 or 512 (plus one producer warp) */
+  int items_per_thread;       /* fact rows per consumer thread per tile: 4, 8 or 16 */
   int stages;                 /* 2..8 bulk-copy stages */
   int grid;                   /* CTAs; 0 = one wave of resident CTAs */
+  int group_mode;             /* 0 auto, 1 groups in shared memory (flushed per CTA), 2 global atomics per row */
 } mb_star_args;
 
 /* Fused filter -> chained probe -> group-by/aggregate over the fact table.

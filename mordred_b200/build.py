@@ -9,13 +9,14 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmordred_b200.so")
 
-SOURCES = ["capi.cu", "star.cu", "build.cu"]
+SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -45,22 +46,36 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    """Compile the library if any source is newer than it; return its path."""
-    if not force and up_to_date():
-        return LIB
-    cmd = [nvcc(), *GENCODE, "-lineinfo", "-O3", "-std=c++17", "--shared",
-           "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-I", os.path.join(ROOT, "include"),
-           "-o", LIB + ".tmp", *_sources(), "-lpthread"]
-    if ptxas_verbose:
-        cmd[1:1] = ["-Xptxas", "-v"]
+def _run(cmd: list[str], verbose: bool) -> str:
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
+    return res.stderr
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    """Compile the library if any source is newer than it; return its path.
+
+    Each translation unit is compiled to an object in parallel, then linked."""
+    if not force and up_to_date():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc(), *GENCODE, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-O3", "-I", os.path.join(ROOT, "include")]
     if ptxas_verbose:
-        print(res.stderr, file=sys.stderr)
+        common += ["-Xptxas", "-v"]
+    jobs = []
+    for src in _sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        jobs.append(([*common, "-c", "-o", obj, src], obj))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        logs = list(ex.map(lambda j: _run(j[0], verbose), jobs))
+    if ptxas_verbose:
+        print("\n".join(logs), file=sys.stderr)
+    _run([nvcc(), *GENCODE, "--shared", "-o", LIB + ".tmp", *[o for _, o in jobs], "-lpthread"], verbose)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

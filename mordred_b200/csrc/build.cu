@@ -110,6 +110,7 @@ using namespace mb;
 extern "C" int mb_build_pht(const int* filter_col, int filter_mode, int c1, int c2, const int* dim_key,
                             const int* dim_val, int num_tuples, int* ht, int num_slots, int key_min,
                             uint32_t* presence, mb_stream_t stream) {
+  if (num_tuples == 0) return MB_OK;
   if (dim_key == nullptr || ht == nullptr || num_tuples < 0 || num_slots <= 0) return MB_ERR_ARG;
   if (filter_col != nullptr && (filter_mode < MB_FILTER_EQ || filter_mode > MB_FILTER_EQ_OR_EQ)) return MB_ERR_ARG;
   if (dim_val != nullptr && !aligned8(ht)) return MB_ERR_ALIGN;
@@ -138,6 +139,7 @@ extern "C" int mb_join_build(const int* dim_key, const int* dim_val, int num_tup
 extern "C" int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_buildArgsGPU* bargs,
                              int num_tuples, int* hash_table, int start_offset, const short* segment_group,
                              mb_stream_t stream) {
+  if (num_tuples == 0) return MB_OK;
   if (bargs == nullptr || bargs->key_idx == nullptr || hash_table == nullptr || num_tuples < 0 ||
       bargs->num_slots <= 0)
     return MB_ERR_ARG;

@@ -145,6 +145,7 @@ int mb_star_query(const mb_star_args* args, mb_stream_t stream) {
 int mb_q11_query(const int* lo_orderdate, const int* lo_discount, const int* lo_quantity,
                  const int* lo_extendedprice, int lo_num_entries, unsigned long long* revenue, int* d_total,
                  mb_stream_t stream) {
+  if (lo_num_entries == 0) return MB_OK;
   if (!lo_orderdate || !lo_discount || !lo_quantity || !lo_extendedprice || !revenue || lo_num_entries < 0)
     return MB_ERR_ARG;
   mb_star_args a;
@@ -212,6 +213,7 @@ int mb_q41_probe(const int* lo_orderdate, const int* lo_partkey, const int* lo_c
 int mb_join_probe(const int* fact_fkey, const int* fact_val, int num_tuples, const int* hash_table, int num_slots,
                   unsigned long long* res, mb_stream_t stream) {
   // src/ops/join.cu:62-73: PHT_2 probe, sum of fact_val * dim_val (int32 product)
+  if (num_tuples == 0) return MB_OK;
   if (!fact_fkey || !fact_val || !hash_table || !res) return MB_ERR_ARG;
   mb_star_args a;
   memset(&a, 0, sizeof(a));
@@ -232,6 +234,7 @@ static int engine_star(const int* gpuCache, const mb_filterArgsGPU* fargs, const
                        const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, int start_offset,
                        const short* segment_group, mb_stream_t stream, bool group_by, bool probe_only_date) {
   if (pargs == nullptr || gargs == nullptr || res == nullptr || num_tuples < 0) return MB_ERR_ARG;
+  if (num_tuples == 0) return MB_OK;
   mb_star_args a;
   memset(&a, 0, sizeof(a));
   a.num_rows = num_tuples;
@@ -315,7 +318,9 @@ int mb_filter_probe_aggr_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs
 // ---- generator ----------------------------------------------------------------------------
 int mb_gen_fact_column(int col, uint64_t seed, int64_t row0, int64_t n, int s_len, int c_len, int p_len, int* out,
                        mb_stream_t stream) {
-  if (!mb_is_fact_column(col) || out == nullptr || n < 0 || row0 < 0) return MB_ERR_ARG;
+  if (!mb_is_fact_column(col) || n < 0 || row0 < 0) return MB_ERR_ARG;
+  if (n == 0) return MB_OK;
+  if (out == nullptr) return MB_ERR_ARG;
   int err = MB_OK;
   DeviceState* ds = current_device_state(&err);
   if (ds == nullptr) return err;
@@ -330,7 +335,9 @@ int mb_gen_fact_column(int col, uint64_t seed, int64_t row0, int64_t n, int s_le
 }
 
 int mb_gen_dim_column(int col, uint64_t seed, int64_t n, int* out, mb_stream_t stream) {
-  if (mb_is_fact_column(col) || out == nullptr || n < 0) return MB_ERR_ARG;
+  if (mb_is_fact_column(col) || n < 0) return MB_ERR_ARG;
+  if (n == 0) return MB_OK;
+  if (out == nullptr) return MB_ERR_ARG;
   int err = MB_OK;
   DeviceState* ds = current_device_state(&err);
   if (ds == nullptr) return err;
@@ -345,7 +352,9 @@ int mb_gen_dim_column(int col, uint64_t seed, int64_t n, int* out, mb_stream_t s
 
 int mb_gen_fact_column_host(int col, uint64_t seed, int64_t row0, int64_t n, int s_len, int c_len, int p_len,
                             int* out, int nthreads) {
-  if (!mb_is_fact_column(col) || out == nullptr || n < 0 || row0 < 0) return MB_ERR_ARG;
+  if (!mb_is_fact_column(col) || n < 0 || row0 < 0) return MB_ERR_ARG;
+  if (n == 0) return MB_OK;
+  if (out == nullptr) return MB_ERR_ARG;
   host_parallel(n, nthreads, [&](long long lo, long long hi) {
     for (long long i = lo; i < hi; ++i)
       out[i] = mb_gen_fact_value(seed, col, static_cast<uint64_t>(row0 + i), s_len, c_len, p_len);
@@ -354,7 +363,9 @@ int mb_gen_fact_column_host(int col, uint64_t seed, int64_t row0, int64_t n, int
 }
 
 int mb_gen_dim_column_host(int col, uint64_t seed, int64_t n, int* out, int nthreads) {
-  if (mb_is_fact_column(col) || out == nullptr || n < 0) return MB_ERR_ARG;
+  if (mb_is_fact_column(col) || n < 0) return MB_ERR_ARG;
+  if (n == 0) return MB_OK;
+  if (out == nullptr) return MB_ERR_ARG;
   host_parallel(n, nthreads, [&](long long lo, long long hi) {
     for (long long i = lo; i < hi; ++i) out[i] = mb_gen_dim_value(seed, col, static_cast<uint64_t>(i));
   });

@@ -1,12 +1,22 @@
 // star.cuh — the fused star-query pipeline: its device-side plan and the host launcher.
 //
-// One persistent kernel runs filter -> chained perfect-hash probes -> group-by /
-// aggregate over the fact table. Fact-column tiles stream into shared memory through
-// 1-D bulk copies (cp.async.bulk, no multicast) in a ring of mbarrier-tracked stages;
-// threads read them back with 128-bit shared loads, keep the selection of their rows
-// as a bitmask, probe L2-resident hash tables (or presence bitmaps staged in shared
-// memory) and accumulate 64-bit sums in registers (scalar) or in a shared-memory group
-// array that is flushed with one 64-bit atomic per touched group per CTA.
+// One persistent, warp-specialised kernel runs filter -> chained perfect-hash probes ->
+// group-by / aggregate over the fact table:
+//   * a producer warp streams fact-column tiles into shared memory with 1-D bulk copies
+//     (cp.async.bulk, no multicast) into a ring of stages, each guarded by a "full"
+//     mbarrier (transaction bytes) and an "empty" mbarrier (one arrival per consumer warp);
+//   * each consumer warp owns a contiguous slice of every tile. A dense phase reads its
+//     rows with 128-bit shared loads and applies the filters and the probes whose
+//     presence bitmap sits in shared memory, keeping the selection as a bitmask; the
+//     survivors are compacted (warp prefix sum) into a per-warp row list, and a sparse
+//     phase runs the remaining L2-resident probes over that list with every lane busy,
+//     issuing the table loads of all remaining probes at once (each probe's slot depends
+//     only on the row's own key) before combining them in the reference's order;
+//   * sums are 64-bit integers in registers (scalar), in a shared-memory group array
+//     flushed with one 64-bit atomic per touched group per CTA, or 64-bit atomics in L2.
+// The query shape (number of filters, of bitmap-decided probes and of table probes) is
+// a template parameter for the common shapes, so their loops unroll to straight code;
+// any other shape runs the same kernel with the counts read from the plan.
 #pragma once
 
 #include "common.cuh"
@@ -29,6 +39,8 @@ struct StarPlan {
   int nf;
   int f_col[MB_MAX_FILTERS], f_mode[MB_MAX_FILTERS], f_c1[MB_MAX_FILTERS], f_c2[MB_MAX_FILTERS];
   int np;
+  int n_dense;                    // leading probes answered by a staged bitmap alone
+  unsigned dense_bias;            // their group terms (0 - min_val) * unique_val, summed
   int p_col[MB_MAX_PROBES];
   const int* p_ht[MB_MAX_PROBES];
   int p_slots[MB_MAX_PROBES], p_kmin[MB_MAX_PROBES], p_layout[MB_MAX_PROBES];
@@ -50,7 +62,7 @@ struct StarPlan {
   int seg_shift;
   unsigned int* status;
   int stages;
-  int smem_groups_off, smem_stage_off, stage_bytes, smem_total;
+  int smem_groups_off, smem_list_off, smem_stage_off, stage_bytes, smem_total;
 };
 
 // Host: validate `a`, fill `plan`, pick the kernel variant and launch it on `stream`.

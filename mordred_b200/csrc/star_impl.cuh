@@ -1,0 +1,514 @@
+// star_impl.cuh — device code of the fused star-query kernel (see star.cuh), shared by
+// the translation units that instantiate its variants.
+//
+// Semantics follow the reference kernels row for row:
+//   filters      GPUProcessing.h:74-86 (fact BETWEEN), crystal/pred.cuh (EQ, EQ OR EQ)
+//   probes       crystal/join.cuh:5-165 (PHT_1 / PHT_2), BlockLibrary.cuh:86-111 (engine)
+//   group index  GPUProcessing.h:143 ((g1-m1)*u1 + ... ) % total_val, int32 arithmetic
+//   aggregate    q11.cu:74 (int32 product widened), GPUProcessing.h:149-150 (int32 difference)
+// Rows are independent and every sum is a 64-bit integer, so the order in which tiles,
+// rows and atomics are applied cannot change any result bit.
+#pragma once
+
+#include "star.cuh"
+
+namespace mb {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// A compiled kernel variant: consumer warps, rows per lane per tile and the query
+// shape it is specialised for (-1 = read from the plan at run time).
+using KernelFn = void (*)(StarPlan);
+struct Variant {
+  int warps, items, nf, nd, ns;
+  KernelFn fn;
+};
+
+__device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
+  if (mode == MB_FILTER_BETWEEN) return x >= c1 && x <= c2;
+  if (mode == MB_FILTER_EQ) return x == c1;
+  return x == c1 || x == c2;
+}
+
+// ((key - key_min) % slots) in 32-bit two's complement (crystal/join.cuh:3); the common
+// in-range case skips the division.
+__device__ __forceinline__ int pht_slot(int key, int slots, int kmin) {
+  const int d = static_cast<int>(static_cast<unsigned>(key) - static_cast<unsigned>(kmin));
+  return (static_cast<unsigned>(d) < static_cast<unsigned>(slots)) ? d : d % slots;
+}
+
+__device__ __forceinline__ bool aligned16_dev(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Column pointer for row `r` of this call (direct or through the segment cache).
+__device__ __forceinline__ const int* row_ptr(const StarPlan& P, int c, long long r) {
+  if (P.gpu_cache == nullptr) return P.col[c] + r;
+  const long long vseg = r >> P.seg_shift;
+  const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg])
+                              : static_cast<int>((P.start_offset + r) >> P.seg_shift);
+  const long long slot = P.col[c][seg];
+  return P.gpu_cache + (slot << P.seg_shift) + (r & ((1ll << P.seg_shift) - 1));
+}
+
+// Survivors gathered from a staged tile through a warp's row list.
+template <int TILE, int R>
+struct GatherLoader {
+  static constexpr int ITEMS = R;
+  const int* wstage;
+  int r[R];
+  __device__ __forceinline__ void load(int c, int (&v)[R]) const {
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = wstage[c * TILE + r[i]];
+  }
+};
+
+// One remainder row read straight from global memory.
+struct RowLoader {
+  static constexpr int ITEMS = 1;
+  const StarPlan* P;
+  long long r;
+  __device__ __forceinline__ void load(int c, int (&v)[1]) const { v[0] = __ldg(row_ptr(*P, c, r)); }
+};
+
+// Key columns of group h from the payloads of table probes p0.. (gv[q] = probe p0 + q).
+// Bitmap-decided probes have payload 0 and the caller zeroed the result, so they are
+// not written.
+template <int NSC, int ITEMS>
+__device__ __forceinline__ void write_keys(const StarPlan& P, int h, const int (&gv)[MB_MAX_PROBES][ITEMS], int i,
+                                           int p0, int ns) {
+  int* res = static_cast<int*>(P.res);
+  const int stride = P.res_layout == MB_RES_ENGINE6 ? 6 : 4;
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= (NSC >= 0 ? NSC : ns)) break;
+    const int rs = P.p_res_slot[p0 + q];
+    if (rs >= 0) res[stride * h + rs] = gv[q][i];
+  }
+}
+
+__device__ __forceinline__ unsigned long long* group_sum_ptr(const StarPlan& P, int h) {
+  if (P.res_layout == MB_RES_ENGINE6)
+    return reinterpret_cast<unsigned long long*>(static_cast<int*>(P.res) + 6 * h + 4);
+  if (P.res_layout == MB_RES_CRYSTAL4)
+    return reinterpret_cast<unsigned long long*>(static_cast<int*>(P.res) + 4 * h + 2);
+  return static_cast<unsigned long long*>(P.res) + h;
+}
+
+struct Accum {
+  unsigned long long acc = 0, cnt = 0;
+  bool bad_probe = false, bad_group = false;
+};
+
+// Aggregate the rows still selected in `sel` into the scalar or the groups. gv[q] is the
+// payload of table probe p0 + q; `bias` already holds the group terms of every probe
+// before p0 (bitmap-decided probes, payload 0).
+template <int NSC, int ITEMS, class L>
+__device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, uint32_t sel,
+                                               const int (&gv)[MB_MAX_PROBES][ITEMS], int p0, int ns,
+                                               unsigned bias, Accum& A, unsigned long long* s_sum,
+                                               uint32_t* s_touch) {
+  int a0[ITEMS], a1[ITEMS];
+  ld.load(P.a_col[0], a0);
+  if (P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL) ld.load(P.a_col[1], a1);
+#pragma unroll
+  for (int i = 0; i < ITEMS; ++i) {
+    if (!(sel & (1u << i))) continue;
+    int val;
+    if (P.agg_op == MB_AGG_SUM)
+      val = a0[i];
+    else if (P.agg_op == MB_AGG_SUB)
+      val = static_cast<int>(static_cast<unsigned>(a0[i]) - static_cast<unsigned>(a1[i]));
+    else if (P.agg_op == MB_AGG_MUL_PAYLOAD)
+      val = static_cast<int>(static_cast<unsigned>(a0[i]) * static_cast<unsigned>(gv[0][i]));
+    else
+      val = static_cast<int>(static_cast<unsigned>(a0[i]) * static_cast<unsigned>(a1[i]));
+    const unsigned long long w = static_cast<unsigned long long>(static_cast<long long>(val));
+    if (P.gmode == kGroupScalar) {
+      A.acc += w;
+      continue;
+    }
+    unsigned hh = bias;
+#pragma unroll
+    for (int q = 0; q < MB_MAX_PROBES; ++q) {
+      if (q >= (NSC >= 0 ? NSC : ns)) break;
+      const int p = p0 + q;
+      hh += (static_cast<unsigned>(gv[q][i]) - static_cast<unsigned>(P.p_min[p])) * static_cast<unsigned>(P.p_mul[p]);
+    }
+    int h = static_cast<int>(hh);
+    if (static_cast<unsigned>(h) >= static_cast<unsigned>(P.total_val)) h = h % P.total_val;
+    if (h < 0) {
+      A.bad_group = true;
+      continue;
+    }
+    if (P.gmode == kGroupSmem) {
+      atomicAdd(&s_sum[h], w);
+      const uint32_t bit = 1u << (h & 31);
+      if (!(s_touch[h >> 5] & bit)) {
+        if (!(atomicOr(&s_touch[h >> 5], bit) & bit) && P.res_layout != MB_RES_DENSE)
+          write_keys<NSC, ITEMS>(P, h, gv, i, p0, ns);
+      }
+    } else {
+      if (P.res_layout != MB_RES_DENSE) write_keys<NSC, ITEMS>(P, h, gv, i, p0, ns);
+      atomicAdd(group_sum_ptr(P, h), w);
+    }
+  }
+}
+
+// Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes. The loads
+// of every probe are issued together; presence is then combined probe by probe in
+// order, so selection, payloads and status bits equal the sequential chain.
+template <int NSC, class L>
+__device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint32_t sel, int p0, int ns,
+                                            unsigned bias, Accum& A, unsigned long long* s_sum, uint32_t* s_touch,
+                                            const unsigned char* smem) {
+  constexpr int ITEMS = L::ITEMS;
+  if (sel == 0) return;
+  int v[ITEMS];
+  int gv[MB_MAX_PROBES][ITEMS];
+  unsigned long long sv[MB_MAX_PROBES][ITEMS];
+  uint32_t range_bad[MB_MAX_PROBES], absent[MB_MAX_PROBES];
+#pragma unroll
+  for (int p = 0; p < MB_MAX_PROBES; ++p) {
+    range_bad[p] = 0;
+    absent[p] = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      gv[p][i] = 0;
+      sv[p][i] = 0;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= (NSC >= 0 ? NSC : ns)) break;
+    const int p = p0 + q;
+    ld.load(P.p_col[p], v);
+    const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
+    const int* ht = P.p_ht[p];
+    const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      if (sel & (1u << i)) {
+        const int h = pht_slot(v[i], slots, kmin);
+        if (h < 0)
+          range_bad[q] |= 1u << i;
+        else if (bm != nullptr && !((bm[h >> 5] >> (h & 31)) & 1u))
+          absent[q] |= 1u << i;
+        else if (layout == MB_HT_KEY)
+          sv[q][i] = bm != nullptr ? 1ull : static_cast<unsigned long long>(static_cast<unsigned>(__ldg(ht + h)));
+        else
+          sv[q][i] = ldg_u64(ht + 2 * h);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= (NSC >= 0 ? NSC : ns)) break;
+    const int p = p0 + q;
+    const int layout = P.p_layout[p];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      if (!(sel & (1u << i))) continue;
+      if (range_bad[q] & (1u << i)) {
+        A.bad_probe = true;
+        sel &= ~(1u << i);
+      } else if ((absent[q] & (1u << i)) || sv[q][i] == 0) {
+        sel &= ~(1u << i);
+      } else {
+        gv[q][i] = layout == MB_HT_KEY_VAL   ? static_cast<int>(sv[q][i] >> 32)
+                   : layout == MB_HT_VAL_OFF ? static_cast<int>(static_cast<unsigned>(sv[q][i]))
+                                             : 0;
+      }
+    }
+  }
+  if (P.count_after < 0) A.cnt += __popc(sel);
+  if (sel == 0) return;
+  aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
+}
+
+// Dense phase over a warp's slice of a staged tile: lane l owns rows (j*32 + l)*4 + e,
+// read with 128-bit shared loads; applies every filter and the leading probes whose
+// presence bitmap is staged. Returns the selection (bit j*4 + e).
+template <int NFC, int NDC, int ITEMS, int TILE>
+__device__ __forceinline__ uint32_t dense_phase(const StarPlan& P, const int* wstage, const unsigned char* smem,
+                                                Accum& A) {
+  const int lane = threadIdx.x & 31;
+  uint32_t sel = ITEMS == 32 ? kFull : ((1u << ITEMS) - 1u);
+  int v[ITEMS];
+  auto load = [&](int c) {
+#pragma unroll
+    for (int j = 0; j < ITEMS / 4; ++j) {
+      const int4 q = lds128(wstage + c * TILE + (j * 32 + lane) * 4);
+      v[4 * j + 0] = q.x;
+      v[4 * j + 1] = q.y;
+      v[4 * j + 2] = q.z;
+      v[4 * j + 3] = q.w;
+    }
+  };
+  const int nf = NFC >= 0 ? NFC : P.nf;
+#pragma unroll
+  for (int f = 0; f < MB_MAX_FILTERS; ++f) {
+    if (f >= nf) break;
+    if (P.count_after == f) A.cnt += __popc(sel);
+    if (f > 0 && !__any_sync(kFull, sel != 0)) continue;
+    load(P.f_col[f]);
+    const int mode = P.f_mode[f], c1 = P.f_c1[f], c2 = P.f_c2[f];
+    if (mode == MB_FILTER_BETWEEN) {
+      // c1 <= x <= c2  <=>  (unsigned)(x - c1) <= (unsigned)(c2 - c1), for c1 <= c2
+      const unsigned span = static_cast<unsigned>(c2) - static_cast<unsigned>(c1);
+      if (c2 < c1) sel = 0;
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i)
+        if (static_cast<unsigned>(v[i]) - static_cast<unsigned>(c1) > span) sel &= ~(1u << i);
+    } else {
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i)
+        if (!pass_filter(v[i], mode, c1, c2)) sel &= ~(1u << i);
+    }
+  }
+  if (P.count_after >= nf) A.cnt += __popc(sel);
+  const int nd = NDC >= 0 ? NDC : P.n_dense;
+#pragma unroll
+  for (int p = 0; p < MB_MAX_PROBES; ++p) {
+    if (p >= nd) break;
+    if ((p > 0 || nf > 0) && !__any_sync(kFull, sel != 0)) break;
+    load(P.p_col[p]);
+    const uint32_t* bm = reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]);
+    const int slots = P.p_slots[p], kmin = P.p_kmin[p];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const int h = pht_slot(v[i], slots, kmin);
+      if (h < 0) {
+        if (sel & (1u << i)) A.bad_probe = true;
+        sel &= ~(1u << i);
+      } else if (!((bm[h >> 5] >> (h & 31)) & 1u)) {
+        sel &= ~(1u << i);
+      }
+    }
+  }
+  return sel;
+}
+
+// Warp prefix sum of the selection counts; writes survivor row offsets to `list`.
+__device__ __forceinline__ int compact(uint32_t sel, uint16_t* list) {
+  const int lane = threadIdx.x & 31;
+  const int c = __popc(sel);
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  int pos = incl - c;
+  __syncwarp();  // the previous tile's readers of `list` are done
+  while (sel) {
+    const int i = __ffs(sel) - 1;
+    sel &= sel - 1;
+    list[pos++] = static_cast<uint16_t>(((i >> 2) * 32 + lane) * 4 + (i & 3));
+  }
+  __syncwarp();
+  return total;
+}
+
+// Generic per-row path (remainder rows): every filter and probe with run-time counts.
+template <class L>
+__device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& A, unsigned long long* s_sum,
+                                         uint32_t* s_touch, const unsigned char* smem) {
+  uint32_t sel = 1u;
+  int v[1];
+  for (int f = 0; f < P.nf; ++f) {
+    if (P.count_after == f) A.cnt += sel;
+    if (!sel) continue;
+    ld.load(P.f_col[f], v);
+    if (!pass_filter(v[0], P.f_mode[f], P.f_c1[f], P.f_c2[f])) sel = 0;
+  }
+  if (P.count_after >= P.nf) A.cnt += sel;
+  // bitmap-decided probes run here as table probes (sparse_rows consults a staged bitmap)
+  sparse_rows<-1>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
+}
+
+template <int NCW, int ITEMS, int NFC, int NDC, int NSC>
+__global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_constant__ StarPlan P) {
+  constexpr int WROWS = 32 * ITEMS;
+  constexpr int TILE = NCW * WROWS;
+  constexpr int NWARPS = NCW + 1;
+  constexpr int R = ITEMS / 4 < 2 ? 2 : ITEMS / 4;  // survivors per lane per sparse round
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ unsigned long long s_red[2 * NWARPS];
+
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + kMaxStages;
+  unsigned long long* s_sum = reinterpret_cast<unsigned long long*>(smem + P.smem_groups_off);
+  uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + P.smem_groups_off + 8 * P.total_val);
+  int* stage_base = reinterpret_cast<int*>(smem + P.smem_stage_off);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int S = P.stages;
+
+  // ---- set-up: group accumulators, staged presence bitmaps, barriers ----------
+  if (P.gmode == kGroupSmem) {
+    for (int g = tid; g < P.total_val; g += NWARPS * 32) s_sum[g] = 0;
+    for (int w = tid; w < (P.total_val + 31) / 32; w += NWARPS * 32) s_touch[w] = 0;
+  }
+  for (int p = 0; p < P.np; ++p) {
+    if (P.p_bm_off[p] < 0) continue;
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem + P.p_bm_off[p]);
+    const int words = P.p_bm_words[p];
+    if (P.p_presence[p] != nullptr) {
+      for (int w = tid; w < words; w += NWARPS * 32) bm[w] = __ldg(P.p_presence[p] + w);
+    } else {
+      // derive presence from an MB_HT_KEY table: each thread folds 32 slots into a word
+      // with its eight 16-byte loads in flight together
+      const int slots = P.p_slots[p];
+      const int* ht = P.p_ht[p];
+      const bool vec = aligned16_dev(ht);
+      for (int w = tid; w < words; w += NWARPS * 32) {
+        uint32_t word = 0;
+        if (vec && (w + 1) * 32 <= slots) {
+          int4 q[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) q[j] = __ldg(reinterpret_cast<const int4*>(ht + w * 32) + j);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            word |= ((q[j].x != 0 ? 1u : 0u) << (4 * j)) | ((q[j].y != 0 ? 1u : 0u) << (4 * j + 1)) |
+                    ((q[j].z != 0 ? 1u : 0u) << (4 * j + 2)) | ((q[j].w != 0 ? 1u : 0u) << (4 * j + 3));
+        } else {
+          for (int j = 0; j < 32 && w * 32 + j < slots; ++j) word |= (__ldg(ht + w * 32 + j) != 0 ? 1u : 0u) << j;
+        }
+        bm[w] = word;
+      }
+    }
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NCW);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  const long long G = gridDim.x;
+  const long long b = blockIdx.x;
+  const long long my_tiles = P.nfull > b ? (P.nfull - 1 - b) / G + 1 : 0;
+  const uint32_t stage_words = static_cast<uint32_t>(P.ncols) * TILE;
+  Accum A;
+  bool failed = false;
+
+  if (warp == 0) {
+    // ---- producer: one lane streams tiles into the stage ring ----------------------
+    if (lane == 0) {
+      const uint64_t policy = l2_policy_evict_first();
+      long long k = 0;
+      for (; k < my_tiles; ++k) {
+        const int s = static_cast<int>(k % S);
+        if (k >= S && !mbar_wait_bounded(&empty[s], static_cast<uint32_t>(((k / S) - 1) & 1))) {
+          failed = true;
+          break;
+        }
+        const long long r0 = (b + k * G) * static_cast<long long>(TILE);
+        int* dst = stage_base + s * stage_words;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&full[s], stage_words * 4u);
+        if (P.gpu_cache == nullptr) {
+          for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, &full[s], policy);
+        } else {
+          const long long vseg = r0 >> P.seg_shift;
+          const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg])
+                                      : static_cast<int>((P.start_offset + r0) >> P.seg_shift);
+          const long long in_seg = r0 & ((1ll << P.seg_shift) - 1);
+          for (int c = 0; c < P.ncols; ++c) {
+            const long long slot = P.col[c][seg];
+            bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, &full[s], policy);
+          }
+        }
+      }
+      // no copy may land after the CTA is gone: wait (bounded) for the last ones issued
+      for (long long j = (k > S ? k - S : 0); j < k; ++j)
+        if (!mbar_wait_bounded(&full[j % S], static_cast<uint32_t>((j / S) & 1))) failed = true;
+    }
+  } else {
+    // ---- consumers ---------------------------------------------------------------------
+    const int cw = warp - 1;
+    uint16_t* list = reinterpret_cast<uint16_t*>(smem + P.smem_list_off) + cw * WROWS;
+    const int nd = NDC >= 0 ? NDC : P.n_dense;
+    const int ns = NSC >= 0 ? NSC : P.np - P.n_dense;
+    const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
+    for (long long k = 0; k < my_tiles; ++k) {
+      const int s = static_cast<int>(k % S);
+      const bool ok = mbar_wait_bounded(&full[s], static_cast<uint32_t>((k / S) & 1));
+      if (!__all_sync(kFull, ok)) {
+        failed = true;
+        break;
+      }
+      const int* wstage = stage_base + s * stage_words + cw * WROWS;
+      const uint32_t sel = dense_phase<NFC, NDC, ITEMS, TILE>(P, wstage, smem, A);
+      const int total = compact(sel, list);
+      for (int base = 0; base < total; base += 32 * R) {
+        GatherLoader<TILE, R> ld;
+        ld.wstage = wstage;
+        uint32_t live = 0;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+          const int idx = base + i * 32 + lane;
+          ld.r[i] = idx < total ? list[idx] : 0;
+          if (idx < total) live |= 1u << i;
+        }
+        sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    // ---- remainder rows (fewer than one tile per CTA), plain loads -----------------
+    if (!failed) {
+      const long long tail0 = P.nfull * TILE;
+      for (long long r = tail0 + b * (NCW * 32) + (tid - 32); r < P.n; r += G * (NCW * 32)) {
+        RowLoader ld{&P, r};
+        tail_row(P, ld, A, s_sum, s_touch, smem);
+      }
+    }
+  }
+
+  if (failed) set_status(P.status, MB_STATUS_TIMEOUT);
+  if (A.bad_probe) set_status(P.status, MB_STATUS_PROBE_RANGE);
+  if (A.bad_group) set_status(P.status, MB_STATUS_GROUP_RANGE);
+
+  // ---- publish -------------------------------------------------------------------
+  unsigned long long acc = A.acc, cnt = A.cnt;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    acc += __shfl_down_sync(kFull, acc, o);
+    cnt += __shfl_down_sync(kFull, cnt, o);
+  }
+  if (lane == 0) {
+    s_red[warp] = acc;
+    s_red[NWARPS + warp] = cnt;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long ta = 0, tc = 0;
+    for (int w = 0; w < NWARPS; ++w) {
+      ta += s_red[w];
+      tc += s_red[NWARPS + w];
+    }
+    if (P.gmode == kGroupScalar && ta != 0) atomicAdd(static_cast<unsigned long long*>(P.res), ta);
+    if (P.count != nullptr && tc != 0) {
+      if (P.count32)
+        atomicAdd(static_cast<int*>(P.count), static_cast<int>(tc));
+      else
+        atomicAdd(static_cast<unsigned long long*>(P.count), tc);
+    }
+  }
+  if (P.gmode == kGroupSmem) {
+    for (int g = tid; g < P.total_val; g += NWARPS * 32)
+      if ((s_touch[g >> 5] >> (g & 31)) & 1u) atomicAdd(group_sum_ptr(P, g), s_sum[g]);
+  }
+}
+
+// Variant tables, one per translation unit that instantiates kernels.
+const Variant* star_variants_generic(int* count);
+const Variant* star_variants_special(int* count);
+
+}  // namespace mb

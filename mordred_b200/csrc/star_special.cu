@@ -1,0 +1,26 @@
+// star_special.cu — kernel variants specialised for the common query shapes
+// (filters, bitmap-decided probes, table probes), in their own translation unit so the
+// build compiles them in parallel with the generic variants.
+#include "star_impl.cuh"
+
+namespace mb {
+
+#define MB_SHAPE_VARIANTS(NF, ND, NS)                                                                  \
+  {4, 16, NF, ND, NS, star_kernel<4, 16, NF, ND, NS>}, {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS>}, \
+      {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS>}, {8, 16, NF, ND, NS, star_kernel<8, 16, NF, ND, NS>}
+
+static const Variant kSpecial[] = {
+    MB_SHAPE_VARIANTS(3, 0, 0),  // filter-aggregate (q11.cu)
+    MB_SHAPE_VARIANTS(0, 1, 2),  // Query A: supplier bitmap, part and date tables (q21.cu)
+    MB_SHAPE_VARIANTS(0, 1, 3),  // Query B: supplier bitmap, customer, part, date (q41.cu)
+    MB_SHAPE_VARIANTS(2, 0, 4),  // engine filter_probe_group_by over four tables
+    MB_SHAPE_VARIANTS(0, 0, 4),  // engine probe_group_by over four tables
+    MB_SHAPE_VARIANTS(0, 0, 1),  // src/ops probe, one table
+};
+
+const Variant* star_variants_special(int* count) {
+  *count = static_cast<int>(sizeof(kSpecial) / sizeof(kSpecial[0]));
+  return kSpecial;
+}
+
+}  // namespace mb

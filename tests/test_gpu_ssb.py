@@ -340,7 +340,7 @@ def _engine_hts(t, s):
     return out
 
 
-@pytest.mark.parametrize("segments", [None, [3, 0, 5, 1], [5], [2, 5, 4]])
+@pytest.mark.parametrize("segments", [None, [3, 0, 1, 5], [5], [2, 4], [4, 0, 2, 3, 1, 5]])
 def test_engine_filter_probe_group_by_segment_cache(segments):
     s, t, cache, col_idx, nseg, lo_len = _engine_setup()
     hts = _engine_hts(t, s)
