@@ -136,11 +136,11 @@ def lib() -> C.CDLL:
         if _lib is None:
             path = lib_path()
             if not os.path.exists(path) or not _build.up_to_date():
+                # a library older than its sources is never used: rebuild or fail
                 try:
                     _build.build()
-                except Exception as e:  # nvcc missing on a box that only has the .so
-                    if not os.path.exists(path):
-                        raise ImportError(f"libmordred_b200.so is not built and cannot be built: {e}")
+                except Exception as e:
+                    raise ImportError(f"libmordred_b200.so is missing or stale and the build failed: {e}")
             l = C.CDLL(path)
             for name, (res, args) in SIGNATURES.items():
                 fn = getattr(l, name)

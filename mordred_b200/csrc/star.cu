@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "star_impl.cuh"
+#include "tuned_configs.h"
 
 namespace mb {
 
@@ -172,8 +173,10 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32) {
   }
 
   // ---- launch configuration and shared-memory plan ------------------------------
-  const int threads = a->threads ? a->threads : 256;
-  const int items = a->items_per_thread ? a->items_per_thread : 8;
+  // Unset fields take the tuned configuration for this query shape (tuned_configs.h).
+  const TunedConfig tc = tuned_config(P.nf, a->num_probes, a->probe[0].layout, P.res_layout, P.total_val);
+  const int threads = a->threads ? a->threads : tc.threads;
+  const int items = a->items_per_thread ? a->items_per_thread : tc.items;
   if (threads % 32 != 0 || threads < 128 || threads > 512) return MB_ERR_ARG;
   if (items != 4 && items != 8 && items != 16) return MB_ERR_ARG;
   const int ncw = threads / 32;
@@ -185,20 +188,21 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32) {
   const bool use_tiles = P.gpu_cache != nullptr || direct_aligned;
   P.nfull = use_tiles ? P.n / tile : 0;
 
+  const int group_mode = a->group_mode ? a->group_mode : tc.group_mode;
   if (P.res_layout == MB_RES_SCALAR)
     P.gmode = kGroupScalar;
-  else if (a->group_mode == 2)
+  else if (group_mode == 2)
     P.gmode = kGroupGlobal;
   else
     P.gmode = P.total_val <= kSmemGroupMax ? kGroupSmem : kGroupGlobal;
-  if (a->group_mode == 1 && P.gmode != kGroupSmem) return MB_ERR_SIZE;
+  if (group_mode == 1 && P.gmode != kGroupSmem) return MB_ERR_SIZE;
 
   const int budget = ds->max_smem_optin - 2048 - 2 * 8 * (ncw + 1);
-  const int want_stages = a->stages ? a->stages : 4;
+  const int want_stages = a->stages ? a->stages : tc.stages;
   if (want_stages < 2 || want_stages > kMaxStages) return MB_ERR_ARG;
   int smem = layout_smem(P, ncw, items, want_stages, true);
   while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);
-  if (smem > budget && P.gmode == kGroupSmem && a->group_mode != 1) {
+  if (smem > budget && P.gmode == kGroupSmem && group_mode != 1) {
     P.gmode = kGroupGlobal;
     smem = layout_smem(P, ncw, items, want_stages, true);
     while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);

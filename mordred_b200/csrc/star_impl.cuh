@@ -30,11 +30,18 @@ __device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
   return x == c1 || x == c2;
 }
 
-// ((key - key_min) % slots) in 32-bit two's complement (crystal/join.cuh:3); the common
-// in-range case skips the division.
+// Out-of-line remainder for the rare keys outside [key_min, key_min + 2*slots): kept as
+// a call so the hot path never carries an if-converted division.
+static __device__ __noinline__ int slow_mod(int d, int m) { return d % m; }
+
+// ((key - key_min) % slots) in 32-bit two's complement (crystal/join.cuh:3). Keys in
+// [key_min, key_min + slots) map to themselves and the next range wraps by one
+// subtraction (a dense 1-based key N lands on slot 0); only other keys divide.
 __device__ __forceinline__ int pht_slot(int key, int slots, int kmin) {
   const int d = static_cast<int>(static_cast<unsigned>(key) - static_cast<unsigned>(kmin));
-  return (static_cast<unsigned>(d) < static_cast<unsigned>(slots)) ? d : d % slots;
+  if (static_cast<unsigned>(d) < static_cast<unsigned>(slots)) return d;
+  if (static_cast<unsigned>(d) < 2u * static_cast<unsigned>(slots) && slots <= (1 << 30)) return d - slots;
+  return slow_mod(d, slots);
 }
 
 __device__ __forceinline__ bool aligned16_dev(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -138,7 +145,7 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
       hh += (static_cast<unsigned>(gv[q][i]) - static_cast<unsigned>(P.p_min[p])) * static_cast<unsigned>(P.p_mul[p]);
     }
     int h = static_cast<int>(hh);
-    if (static_cast<unsigned>(h) >= static_cast<unsigned>(P.total_val)) h = h % P.total_val;
+    if (static_cast<unsigned>(h) >= static_cast<unsigned>(P.total_val)) h = slow_mod(h, P.total_val);
     if (h < 0) {
       A.bad_group = true;
       continue;
@@ -402,9 +409,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     if (lane == 0) {
       const uint64_t policy = l2_policy_evict_first();
       long long k = 0;
+      int s = 0;
+      uint32_t phase = 0;  // use count of stage s, mod 2
       for (; k < my_tiles; ++k) {
-        const int s = static_cast<int>(k % S);
-        if (k >= S && !mbar_wait_bounded(&empty[s], static_cast<uint32_t>(((k / S) - 1) & 1))) {
+        if (k >= S && !mbar_wait_bounded(&empty[s], phase ^ 1u)) {
           failed = true;
           break;
         }
@@ -424,6 +432,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
             bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, &full[s], policy);
           }
         }
+        if (++s == S) {
+          s = 0;
+          phase ^= 1u;
+        }
       }
       // no copy may land after the CTA is gone: wait (bounded) for the last ones issued
       for (long long j = (k > S ? k - S : 0); j < k; ++j)
@@ -436,9 +448,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     const int nd = NDC >= 0 ? NDC : P.n_dense;
     const int ns = NSC >= 0 ? NSC : P.np - P.n_dense;
     const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
+    int s = 0;
+    uint32_t phase = 0;
     for (long long k = 0; k < my_tiles; ++k) {
-      const int s = static_cast<int>(k % S);
-      const bool ok = mbar_wait_bounded(&full[s], static_cast<uint32_t>((k / S) & 1));
+      const bool ok = mbar_wait_bounded(&full[s], phase);
       if (!__all_sync(kFull, ok)) {
         failed = true;
         break;
@@ -460,6 +473,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
+      if (++s == S) {
+        s = 0;
+        phase ^= 1u;
+      }
     }
     // ---- remainder rows (fewer than one tile per CTA), plain loads -----------------
     if (!failed) {

@@ -1,0 +1,38 @@
+// tuned_configs.h — launch configuration defaults of the fused star kernel per query
+// shape, written by mordred_b200/autotune.py from sweeps on a B200 (threads x rows per
+// thread x stages x group mode, 120,000,000-row fact table). A shape is keyed by its
+// filter count, probe count, first probe's table layout, whether it groups, and whether
+// its group array is large (> 2,048 groups). Unknown shapes take kDefaultConfig.
+#pragma once
+
+namespace mb {
+
+struct TunedConfig {
+  int threads, items, stages, group_mode;
+};
+
+struct TunedEntry {
+  int nf, np, p0_layout, grouped, big_groups;
+  TunedConfig cfg;
+};
+
+static const TunedConfig kDefaultConfig = {256, 8, 2, 0};
+
+static const TunedEntry kTuned[] = {
+    {3, 0, -1, 0, 0, {512, 8, 3, 0}},  // filter-aggregate (q11 form): 0.274 ms, 7.02 TB/s
+    {0, 3, 0, 1, 1, {256, 8, 2, 2}},   // Query A form: 0.489 ms, 3.93 TB/s
+    {0, 4, 0, 1, 0, {256, 8, 2, 0}},   // Query B form: 0.768 ms, 3.75 TB/s
+};
+
+inline TunedConfig tuned_config(int nf, int np, int p0_layout, int res_layout, int total_val) {
+  const int grouped = res_layout != 0 ? 1 : 0;
+  const int big = grouped && total_val > 2048 ? 1 : 0;
+  const int l0 = np > 0 ? p0_layout : -1;
+  for (const TunedEntry& e : kTuned)
+    if (e.nf == nf && e.np == np && e.p0_layout == l0 && e.grouped == grouped && e.big_groups == big) return e.cfg;
+  TunedConfig c = kDefaultConfig;
+  if (big) c.group_mode = 2;  // large group arrays: L2 atomics keep shared memory for stages
+  return c;
+}
+
+}  // namespace mb
