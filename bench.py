@@ -264,7 +264,7 @@ def main():
 
     # ---- roofline of the dominant kernel (the Query B probe: 24 B/row) ---------------------
     peak, peak_kind = measured_peaks()
-    pa, pb = statistics.mean(probe_ms["A"]), statistics.mean(probe_ms["B"])
+    pa, pb = statistics.median(probe_ms["A"]), statistics.median(probe_ms["B"])
     dom = "B" if pb >= pa else "A"
     bytes_dom = n * (QB_BYTES_PER_ROW if dom == "B" else QA_BYTES_PER_ROW)
     achieved = bytes_dom / (pb if dom == "B" else pa) / 1e6  # bytes per ms -> GB/s
