@@ -170,6 +170,25 @@ int mb_q41_probe(const int* lo_orderdate, const int* lo_partkey, const int* lo_c
                  const int* ht_c, int c_len, const int* ht_d, int d_len, int* res,
                  mb_stream_t stream);
 
+/* The Query B probe of mb_q41_probe (same arguments, same result) for callers that
+ * cannot let a library allocate device memory — an executor that sizes every device
+ * buffer in its own arena up front, or a thread that must not take cudaMalloc's
+ * device-wide synchronisation. It has no counterpart in the reference. Its scratch (the
+ * status word and the supplier table's presence bitmap) is a fixed 33,024-byte array in
+ * the library's device image, present on every device that loads the library until
+ * the process exits; nothing is allocated. The first call on a device sets up (device
+ * limits, kernel attributes, the array's device address) with that device current;
+ * make that first call before any stream capture. s_len above 262,144 returns
+ * MB_ERR_SIZE. Every call reuses the one array: the status word is cleared at the start
+ * of each call, and calls whose work overlaps on the GPU (other streams, other host
+ * threads) race on it — serialise them. status (optional, device word) receives the
+ * call's MB_STATUS_* bits. */
+int mb_q41_probe_noalloc(const int* lo_orderdate, const int* lo_partkey, const int* lo_custkey,
+                         const int* lo_suppkey, const int* lo_revenue, const int* lo_supplycost,
+                         int lo_len, const int* ht_p, int p_len, const int* ht_s, int s_len,
+                         const int* ht_c, int c_len, const int* ht_d, int d_len, int* res,
+                         unsigned int* status, mb_stream_t stream);
+
 /* ---- engine (src/gpudb) kernel arguments, restated as plain C ------------------- */
 /* KernelArgs.h:270-286 filterArgsGPU; device predicate function pointers become mode1/mode2. */
 typedef struct mb_filterArgsGPU {

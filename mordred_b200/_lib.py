@@ -97,6 +97,7 @@ SIGNATURES = {
     "mb_q11_query": (I, [P, P, P, P, I, P, P, P]),
     "mb_q21_probe": (I, [P, P, P, P, I, P, I, P, I, P, I, P, P]),
     "mb_q41_probe": (I, [P, P, P, P, P, P, I, P, I, P, I, P, I, P, I, P, P]),
+    "mb_q41_probe_noalloc": (I, [P, P, P, P, P, P, I, P, I, P, I, P, I, P, I, P, P, P]),
     "mb_filter_probe_group_by_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbProbeArgsGPU),
                                           PS(MbGroupbyArgsGPU), I, P, I, P, P]),
     "mb_probe_group_by_GPU2": (I, [P, PS(MbProbeArgsGPU), PS(MbGroupbyArgsGPU), I, P, I, P, P]),

@@ -97,7 +97,7 @@ static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_b
   return P.smem_total;
 }
 
-int launch_star(const mb_star_args* a, cudaStream_t stream, int count32) {
+int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const DeviceState* preset) {
   if (a == nullptr) return MB_ERR_ARG;
   if (a->num_rows < 0) return MB_ERR_ARG;
   if (a->num_rows == 0) return MB_OK;  // empty input: nothing to add (pointers may be null)
@@ -116,7 +116,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32) {
   if (a->group_mode < 0 || a->group_mode > 2) return MB_ERR_ARG;
 
   int err = MB_OK;
-  DeviceState* ds = current_device_state(&err);
+  const DeviceState* ds = preset != nullptr ? preset : current_device_state(&err);
   if (ds == nullptr) return err;
 
   StarPlan P;

@@ -66,8 +66,9 @@ struct StarPlan {
 };
 
 // Host: validate `a`, fill `plan`, pick the kernel variant and launch it on `stream`.
-// count32 makes `count` an int* accumulator.
-int launch_star(const mb_star_args* a, cudaStream_t stream, int count32);
+// count32 makes `count` an int* accumulator. `preset` supplies the device state (SM
+// count, shared-memory limit, status word) instead of the library's own.
+int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const DeviceState* preset = nullptr);
 
 // Host: set per-device kernel attributes (dynamic shared memory opt-in).
 int star_init_device(const DeviceState& ds);
