@@ -249,6 +249,84 @@ int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs,
                   const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table,
                   int start_offset, const short* segment_group, mb_stream_t stream);
 
+/* ---- batched multi-query execution ------------------------------------------------ */
+/* Many star queries over one resident fact table in one launch: every fact tile is
+ * loaded once, each dimension is read once per row through a packed attribute table
+ * (PAT: one 32-bit word per hash slot holding the dimension row's attributes, bit 31 =
+ * row present), and every query of the batch evaluates its range predicates and
+ * aggregate on that shared row. Each query's result equals running it alone through
+ * mb_star_query with per-query filtered hash tables (the reference runs one query at a
+ * time: src/gpudb/QueryProcessing.cu:1347-1471). No counterpart kernel exists in the
+ * reference. */
+#define MB_BATCH_MAX_QUERIES 256
+#define MB_BATCH_MAX_PREDS 4
+
+/* Row schema: fact columns 0..8, then the four dimension words. */
+#define MB_COL_ORDERDATE 0
+#define MB_COL_QUANTITY 1
+#define MB_COL_DISCOUNT 2
+#define MB_COL_EXTENDEDPRICE 3
+#define MB_COL_SUPPKEY 4
+#define MB_COL_CUSTKEY 5
+#define MB_COL_PARTKEY 6
+#define MB_COL_REVENUE 7
+#define MB_COL_SUPPLYCOST 8
+#define MB_COL_DIM_S 9   /* supplier word, looked up by suppkey */
+#define MB_COL_DIM_C 10  /* customer word, by custkey */
+#define MB_COL_DIM_P 11  /* part word, by partkey */
+#define MB_COL_DIM_D 12  /* date word, by orderdate */
+#define MB_NUM_FACT_COLS 9
+/* A field: `width` bits at `shift` of column `col` (width 32 = the whole signed value). */
+#define MB_FIELD(col, shift, width) (((col) << 11) | ((shift) << 6) | (width))
+
+typedef struct mb_pat {
+  const unsigned int* words;  /* words[(key - key_min) % slots] */
+  int slots, key_min;
+} mb_pat;
+
+typedef struct mb_batch_query {
+  int num_preds;                          /* lo <= field <= hi, all must hold */
+  int pred_field[MB_BATCH_MAX_PREDS];
+  int pred_lo[MB_BATCH_MAX_PREDS], pred_hi[MB_BATCH_MAX_PREDS];
+  int dims_required;                      /* bit d: the row's dimension d (S,C,P,D) must exist */
+  int agg_op;                             /* MB_AGG_SUM / SUB / MUL over agg_field[0..1] */
+  int agg_field[2];
+  int num_keys;                           /* group index = sum (key - key_min) * key_mul % total_val */
+  int key_field[2], key_min[2], key_mul[2];
+  int total_val;
+  int res_layout;                         /* MB_RES_SCALAR, MB_RES_CRYSTAL4 (keys 0,1 stored) or MB_RES_DENSE */
+  void* res;                              /* zeroed by the caller; accumulated into */
+} mb_batch_query;
+
+typedef struct mb_batch_args {
+  int64_t num_rows;
+  const int* fact[MB_NUM_FACT_COLS];      /* device columns by MB_COL_* (NULL where unused) */
+  mb_pat dim[4];                          /* S, C, P, D */
+  int num_queries;                        /* 1 .. MB_BATCH_MAX_QUERIES */
+  const mb_batch_query* queries;          /* host array, copied into the launch */
+  void* workspace;                        /* device, >= mb_batch_workspace_bytes(), 16-byte aligned */
+  size_t workspace_bytes;
+  int threads, items_per_thread, stages, grid;  /* 0 = tuned default */
+  int smem_group_bytes;                   /* shared memory for small group arrays; -1 default, 0 none */
+} mb_batch_args;
+
+/* Build a PAT: for each dimension row i, words[(key[i] - key_min) % slots] =
+ * 0x80000000 | attr0 << shift0 | attr1 << shift1 | attr2 << shift2 for the fields
+ * (MB_FIELD(.., shift, width)) given; attributes must fit their widths (else
+ * MB_STATUS_GROUP_RANGE is set and the row is stored without them). words is zeroed by
+ * the caller. */
+int mb_pat_build(const int* dim_key, int num_rows, int key_min, int slots,
+                 const int* attr0, int field0, const int* attr1, int field1,
+                 const int* attr2, int field2, unsigned int* words, mb_stream_t stream);
+
+/* Device workspace the batch needs: for every predicate attribute, a table mapping each
+ * value of the queries' range hull to the bitmask of queries that accept it. */
+size_t mb_batch_workspace_bytes(const mb_batch_args* args);
+
+/* Run a batch of queries: one small kernel fills the workspace's query masks, then one
+ * persistent kernel scans the fact table once. */
+int mb_batch_run(const mb_batch_args* args, mb_stream_t stream);
+
 /* ---- synthetic data (seeded; identical on host and device) ---------------------- */
 /* Fact column `col` (MB_LO_* in mordred_b200/csrc/ssbgen.h) rows [row0, row0+n) into a
  * device buffer. s_len/c_len/p_len give the foreign-key ranges. */

@@ -169,3 +169,41 @@ def device_status(device: int = -1, clear: bool = True) -> int:
 
 def launch_count() -> int:
     return int(lib().mb_launch_count())
+
+
+# ---- batched multi-query (include/mordred_b200.h) ------------------------------------
+MB_BATCH_MAX_QUERIES, MB_BATCH_MAX_PREDS = 256, 4
+(MB_COL_ORDERDATE, MB_COL_QUANTITY, MB_COL_DISCOUNT, MB_COL_EXTENDEDPRICE, MB_COL_SUPPKEY, MB_COL_CUSTKEY,
+ MB_COL_PARTKEY, MB_COL_REVENUE, MB_COL_SUPPLYCOST, MB_COL_DIM_S, MB_COL_DIM_C, MB_COL_DIM_P,
+ MB_COL_DIM_D) = range(13)
+MB_NUM_FACT_COLS = 9
+
+
+def MB_FIELD(col: int, shift: int, width: int) -> int:
+    return (col << 11) | (shift << 6) | width
+
+
+class MbPat(C.Structure):
+    _fields_ = [("words", C.c_void_p), ("slots", C.c_int), ("key_min", C.c_int)]
+
+
+class MbBatchQuery(C.Structure):
+    _fields_ = [("num_preds", C.c_int), ("pred_field", C.c_int * MB_BATCH_MAX_PREDS),
+                ("pred_lo", C.c_int * MB_BATCH_MAX_PREDS), ("pred_hi", C.c_int * MB_BATCH_MAX_PREDS),
+                ("dims_required", C.c_int), ("agg_op", C.c_int), ("agg_field", C.c_int * 2),
+                ("num_keys", C.c_int), ("key_field", C.c_int * 2), ("key_min", C.c_int * 2),
+                ("key_mul", C.c_int * 2), ("total_val", C.c_int), ("res_layout", C.c_int), ("res", C.c_void_p)]
+
+
+class MbBatchArgs(C.Structure):
+    _fields_ = [("num_rows", C.c_int64), ("fact", C.c_void_p * MB_NUM_FACT_COLS), ("dim", MbPat * 4),
+                ("num_queries", C.c_int), ("queries", C.POINTER(MbBatchQuery)), ("workspace", C.c_void_p),
+                ("workspace_bytes", C.c_size_t), ("threads", C.c_int), ("items_per_thread", C.c_int),
+                ("stages", C.c_int), ("grid", C.c_int), ("smem_group_bytes", C.c_int)]
+
+
+SIGNATURES.update({
+    "mb_pat_build": (I, [P, I, I, I, P, I, P, I, P, I, P, P]),
+    "mb_batch_workspace_bytes": (C.c_size_t, [PS(MbBatchArgs)]),
+    "mb_batch_run": (I, [PS(MbBatchArgs), P]),
+})

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmordred_b200.so")
 
-SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "noalloc.cu", "batch.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -33,6 +33,7 @@ static int init_device_locked(int dev) {
   ds.max_smem_optin = optin;
   ds.status = status;
   int e = star_init_device(ds);
+  if (e == MB_OK) e = batch_init_device(ds);
   if (e != MB_OK) return e;
   ds.device = dev;
   return MB_OK;

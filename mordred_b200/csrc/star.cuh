@@ -72,5 +72,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
 
 // Host: set per-device kernel attributes (dynamic shared memory opt-in).
 int star_init_device(const DeviceState& ds);
+// Host: the same for the batched multi-query kernel (batch.cu).
+int batch_init_device(const DeviceState& ds);
 
 }  // namespace mb

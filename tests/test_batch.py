@@ -1,0 +1,102 @@
+"""Batched multi-query execution: the workload generator (CPU) and, on the GPU, every
+query of a batch against the same query run alone (bit for bit) and against the oracle."""
+import numpy as np
+import pytest
+
+from mordred_b200 import batch as B
+from mordred_b200 import ssb
+
+
+def test_generator_is_seeded_and_spans_selectivities():
+    a = B.generate_queries(300, seed=7)
+    b = B.generate_queries(300, seed=7)
+    assert [(q.template, q.date, q.s_region, q.category) for q in a] == \
+           [(q.template, q.date, q.s_region, q.category) for q in b]
+    assert {q.template for q in a} == {"agg", "qa", "qb"}
+    sels = np.array([q.meta["expected_selectivity"] for q in a])
+    assert sels.min() < 1e-3 and sels.max() > 0.05
+    for q in a:
+        assert q.date[0] <= q.date[1] and q.date[0] in B.CALENDAR and q.date[1] in B.CALENDAR
+        assert 0 <= q.s_region[0] <= q.s_region[1] <= 4 and 0 <= q.category[0] <= q.category[1] <= 24
+        assert 1 <= q.quantity[0] <= q.quantity[1] <= 50 and 0 <= q.discount[0] <= q.discount[1] <= 10
+    assert {q.groups for q in a} == {1, 175, 7000}
+
+
+def test_descriptor_fields_fit_the_encoding():
+    for q in B.generate_queries(30, seed=1):
+        c = q.to_c(type("R", (), {"data_ptr": lambda self: 4096})())
+        assert 1 <= c.num_preds <= 4
+        for i in range(c.num_preds):
+            assert 0 <= c.pred_field[i] < 65536 and c.pred_lo[i] <= c.pred_hi[i]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_rows,n_queries", [(1_000_003, 40), (4_194_304, 96)])
+def test_batch_equals_alone(n_rows, n_queries):
+    import torch
+    from mordred_b200 import _lib as L
+    torch.cuda.set_device(0)
+    s = ssb.Sizes(lo_len=n_rows, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(s, 314, B.BATCH_FACT, B.BATCH_DIMS)
+    pats = B.build_pats(t, s)
+    qs = B.generate_queries(n_queries, seed=n_queries, sel_lo=1e-4, sel_hi=0.5)
+    res_b = [q.result_buffer() for q in qs]
+    B.run_batch(t, pats, qs, res_b, n_rows)
+    ws = B.AloneWorkspace(s)
+    for i, q in enumerate(qs):
+        r = q.result_buffer()
+        B.run_alone(t, ws, q, r, n_rows)
+        assert np.array_equal(res_b[i].cpu().numpy(), r.cpu().numpy()), (i, q.template)
+    assert L.device_status(0) == 0
+    assert sum(1 for r in res_b if r.abs().sum().item() != 0) > n_queries // 2
+
+
+@pytest.mark.gpu
+def test_batch_launch_configs_and_oracle():
+    import torch
+    from mordred_b200 import _lib as L
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    n = 600_011
+    s = ssb.Sizes(lo_len=n, s_len=2_000, c_len=30_000, p_len=20_000)
+    t = ssb.gen_device(s, 99, B.BATCH_FACT, B.BATCH_DIMS)
+    pats = B.build_pats(t, s)
+    qs = B.generate_queries(24, seed=3, sel_lo=1e-3, sel_hi=0.5)
+    base = [q.result_buffer() for q in qs]
+    B.run_batch(t, pats, qs, base, n)
+    for threads in (128, 256, 512):
+        for items in (4, 8):
+            for stages in (2, 3):
+                res = [q.result_buffer() for q in qs]
+                try:
+                    B.run_batch(t, pats, qs, res, n, threads=threads, items=items, stages=stages)
+                except L.MbError as e:
+                    # MB_ERR_SIZE: the stage ring does not fit; MB_ERR_ARG: no such compiled variant
+                    assert e.code in (1, 6)
+                    continue
+                for a, b in zip(res, base):
+                    assert torch.equal(a, b), (threads, items, stages)
+    # oracle: the same query through the CPU pipeline with filtered tables
+    h = {k: v.cpu().numpy() for k, v in t.items()}
+    for q, r in zip(qs, base):
+        if q.template != "qb":
+            continue
+        hts = {}
+        for name, key, val, flt, lo, hi, slots, kmin, layout in [
+            ("s", "s_suppkey", None, "s_region", *q.s_region, s.s_len, 0, 0),
+            ("c", "c_custkey", "c_nation", "c_region", *q.c_region, s.c_len, 0, 1),
+            ("p", "p_partkey", None, "p_mfgr", *q.mfgr, s.p_len, 0, 0),
+            ("d", "d_datekey", "d_year", None, 0, 0, ssb.DATE_SLOTS, ssb.DATE_MIN, 1)]:
+            ht = np.zeros(2 * slots, np.int32)
+            O.build_ht(h[flt] if flt else None, 1, lo, hi, h[key], h[val] if val else None, ht, slots, kmin, layout)
+            hts[name] = ht
+        exp = np.zeros(4 * ssb.QB_GROUPS, np.int32)
+        O.star(n, filters=[dict(col=h["lo_orderdate"], mode=1, c1=q.date[0], c2=q.date[1])],
+               probes=[dict(fkey=h["lo_suppkey"], ht=hts["s"], num_slots=s.s_len, layout=0),
+                       dict(fkey=h["lo_custkey"], ht=hts["c"], num_slots=s.c_len, layout=1, unique_val=7, res_slot=1),
+                       dict(fkey=h["lo_partkey"], ht=hts["p"], num_slots=s.p_len, layout=0),
+                       dict(fkey=h["lo_orderdate"], ht=hts["d"], num_slots=ssb.DATE_SLOTS, key_min=ssb.DATE_MIN,
+                            layout=1, min_val=1992, unique_val=1, res_slot=0)],
+               aggr=[h["lo_revenue"], h["lo_supplycost"]], agg_op=1, total_val=ssb.QB_GROUPS, res_layout=2, res=exp)
+        assert np.array_equal(r.cpu().numpy(), exp)
+    assert L.device_status(0) == 0
