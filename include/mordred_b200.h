@@ -306,7 +306,9 @@ typedef struct mb_batch_args {
   const mb_batch_query* queries;          /* host array, copied into the launch */
   void* workspace;                        /* device, >= mb_batch_workspace_bytes(), 16-byte aligned */
   size_t workspace_bytes;
-  int threads, items_per_thread, stages, grid;  /* 0 = tuned default */
+  /* consumer threads x rows per thread per stage: 256x4, 512x4, 512x2, 768x1, 768x2 or
+   * 960x1 (0 = default 768x1); stages 2..8 (0 = 2); grid 0 = one CTA per SM */
+  int threads, items_per_thread, stages, grid;
   int smem_group_bytes;                   /* shared memory for small group arrays; -1 default, 0 none */
 } mb_batch_args;
 

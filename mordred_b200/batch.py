@@ -58,6 +58,7 @@ class Query:
     mfgr: tuple[int, int] = (0, 4)
     target_selectivity: float = 1.0
     meta: dict = field(default_factory=dict)
+    extra: list = field(default_factory=list)  # further (field code, lo, hi) predicates
 
     @property
     def groups(self) -> int:
@@ -92,6 +93,9 @@ class Query:
             q.key_field[0], q.key_min[0], q.key_mul[0] = D_YEAR, 1992, 1
             q.key_field[1], q.key_min[1], q.key_mul[1] = C_NATION, 0, 7
             q.total_val, q.res_layout = ssb.QB_GROUPS, L.MB_RES_CRYSTAL4
+        preds += list(self.extra)
+        if len(preds) > L.MB_BATCH_MAX_PREDS:
+            raise ValueError(f"{len(preds)} predicates; at most {L.MB_BATCH_MAX_PREDS}")
         q.num_preds = len(preds)
         for i, (f, lo, hi) in enumerate(preds):
             q.pred_field[i], q.pred_lo[i], q.pred_hi[i] = f, lo, hi

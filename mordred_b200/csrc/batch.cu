@@ -12,13 +12,15 @@
 //     accept every value), and a table over the 16 dimension-presence patterns does the
 //     same for the dimensions each query needs; a row ANDs one mask per attribute and
 //     visits only the queries left set;
-//   * a visited (row, query) pair adds its 64-bit value to the query's scalar (shared
-//     memory), its shared-memory group array (small group counts, flushed once per CTA)
-//     or its group array in L2.
+//   * the (row, query) pairs a warp finds go to a list in shared memory; a full list is
+//     aggregated 32 pairs at a time, one per lane, by branch-light code driven by a
+//     32-byte per-query descriptor: the pair's 64-bit value is added to the query's
+//     scalar or shared-memory group array (flushed once per CTA) or its group array in L2.
 // A query's result equals its lone run through mb_star_query with filtered hash tables:
 // with unique dimension keys, "the key is in the filtered table" is "the row's
 // attributes pass the filter", and the payload is the attribute itself; sums are
 // integers, so the order of additions cannot change a bit.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -31,27 +33,44 @@ constexpr int kBatchStages = 8;
 constexpr int kMaxPredFields = 8;
 constexpr int kMaskWordsMax = MB_BATCH_MAX_QUERIES / 32;
 constexpr int kSmemTableMaxEntries = 512;  // predicate tables up to this many values sit in shared memory
-constexpr int kMatchListCap = 1024;        // (row, query) pairs a consumer warp collects before aggregating
+constexpr int kMatchListMax = 1024;        // (row, query) pairs a consumer warp collects before aggregating
+constexpr int kColPad = 4;                 // words between staged columns: the same row of two columns
+                                           // falls in different banks (and stays 16-byte aligned)
+constexpr int kMaxStageCols = MB_NUM_FACT_COLS + 1;
+constexpr int kMaxBreakpoints = 768;       // range end points of wide attributes, over all of them
+constexpr int kMaxBuckets = 2048;          // bucket index entries per wide attribute
 
-// Compact per-query descriptor carried in the launch parameters (88 bytes).
+// Field codes inside the kernel address staged columns: (stage column << 11) | (shift << 6) | width.
+// Aggregation descriptor of one query (32 bytes, shared memory). The group index is
+// k0*kmul0 + k1*kmul1 + bias in 32-bit wrapping arithmetic, which equals
+// (k0 - kmin0)*kmul0 + (k1 - kmin1)*kmul1 with bias = -(kmin0*kmul0 + kmin1*kmul1); an
+// absent key has multiplier 0. Scalars are one-group arrays.
+struct __align__(16) AQ {
+  uint16_t a0, a1, k0, k1;  // stage field codes
+  unsigned kmul0, kmul1, bias;
+  int total;                // groups (1 for a scalar)
+  int soff;                 // shared-memory byte offset of the 64-bit sums, -1: atomics in L2
+  int flags;                // bits 0-1 agg op, bit 2 CRYSTAL4 keys, bits 3-4 number of keys
+};
+static_assert(sizeof(AQ) == 32, "aggregation descriptor size");
+
+// Per-query descriptor in the launch parameters (96 bytes).
 struct BQ {
-  uint8_t np, nk, agg_op, res_layout;
-  uint8_t req, pad[3];
-  uint16_t pf[MB_BATCH_MAX_PREDS];
+  AQ a;
+  uint8_t np, res_layout, pad[2];
+  uint16_t pf[MB_BATCH_MAX_PREDS];  // row-schema field codes of the predicates
   int plo[MB_BATCH_MAX_PREDS], phi[MB_BATCH_MAX_PREDS];
-  uint16_t af[2], kf[2];
-  int kmin[2], kmul[2];
-  int total_val;
-  int smem_off;  // byte offset of this query's shared-memory group array, -1 = L2 atomics
+  int pad2;
   void* res;
 };
-static_assert(sizeof(BQ) == 88, "descriptor size");
+static_assert(sizeof(BQ) == 96, "descriptor size");
 
 struct BatchPlan {
   long long n, nfull;
   int ncols;                       // staged fact columns
   const int* col[MB_NUM_FACT_COLS];
   int cidx[13];                    // row-schema column -> stage column (-1: absent)
+  int stage_dim[kMaxStageCols];    // stage column -> dimension whose word it holds (-1: fact column)
   int ndims;
   int dim_list[4];
   int key_stage[4];
@@ -59,15 +78,25 @@ struct BatchPlan {
   int pat_slots[4], pat_kmin[4];
   int nq, nwords;
   int nfields;                     // attributes some query constrains
-  int f_code[kMaxPredFields], f_min[kMaxPredFields], f_n[kMaxPredFields];
+  int f_code[kMaxPredFields], f_scode[kMaxPredFields], f_min[kMaxPredFields], f_n[kMaxPredFields];
   int f_smem_off[kMaxPredFields];  // byte offset of the table in shared memory, -1: workspace
   long long f_goff[kMaxPredFields];// word offset of the table in the workspace
+  int f_ent[kMaxPredFields];       // table entries: f_n, or f_nint for an interval-coded attribute
+  // Interval coding of a wide attribute (hull wider than kSmemTableMaxEntries values): the
+  // queries' range end points cut the hull into f_nint intervals on which every query's
+  // verdict is constant; the table holds one mask per interval. A value v (relative to
+  // f_min) is in interval i when bp[i] <= v < bp[i+1]; bucket v >> f_shift of a shared-
+  // memory index gives the interval of the bucket's first value, and a short forward
+  // scan over the end points finishes the search.
+  int f_nint[kMaxPredFields], f_bp_off[kMaxPredFields], f_shift[kMaxPredFields];
+  int f_bps_off[kMaxPredFields], f_bkt_off[kMaxPredFields];  // shared-memory byte offsets
+  int bp[kMaxBreakpoints];
   unsigned outside[kMaxPredFields][kMaskWordsMax];  // mask for values outside the hull
   unsigned pres_mask[16][kMaskWordsMax];
   unsigned* tables;                // workspace
   long long table_entries;
-  int stages, stage_words;
-  int smem_acc_off, smem_desc_off, smem_pres_off, smem_out_off, smem_tab_off, smem_tab_words, smem_list_off;
+  int stages, stage_words, list_cap;
+  int smem_acc_off, smem_aq_off, smem_res_off, smem_pres_off, smem_out_off, smem_list_off;
   int smem_groups_off, smem_groups_words, smem_stage_off;
   unsigned int* status;
   const int* fact_all[MB_NUM_FACT_COLS];
@@ -84,74 +113,69 @@ __device__ __forceinline__ int bslot(int key, int slots, int kmin) {
 
 __device__ __forceinline__ int field_value(int v, int code) {
   const int width = code & 63;
-  if (width >= 32) return v;
-  const int shift = (code >> 6) & 31;
-  return static_cast<int>((static_cast<unsigned>(v) >> shift) & ((1u << width) - 1u));
+  const unsigned shift = (code >> 6) & 31;
+  const unsigned mask = width >= 32 ? 0xffffffffu : (1u << width) - 1u;
+  return static_cast<int>((static_cast<unsigned>(v) >> shift) & mask);
 }
 
 __device__ __forceinline__ void bmbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long batch_value(const BQ& Q, int a0, int a1) {
-  int v;
-  if (Q.agg_op == MB_AGG_SUM)
-    v = a0;
-  else if (Q.agg_op == MB_AGG_SUB)
-    v = static_cast<int>(static_cast<unsigned>(a0) - static_cast<unsigned>(a1));
-  else
-    v = static_cast<int>(static_cast<unsigned>(a0) * static_cast<unsigned>(a1));
-  return static_cast<unsigned long long>(static_cast<long long>(v));
-}
-
-__device__ __forceinline__ unsigned long long* batch_sum_ptr(const BQ& Q, int g) {
-  if (Q.res_layout == MB_RES_CRYSTAL4) return reinterpret_cast<unsigned long long*>(static_cast<int*>(Q.res) + 4 * g + 2);
-  return static_cast<unsigned long long*>(Q.res) + g;
+__device__ __forceinline__ AQ load_aq(const AQ* s_aq, int qi) {
+  const uint4* p = reinterpret_cast<const uint4*>(s_aq + qi);
+  const uint4 x = p[0], y = p[1];
+  AQ a;
+  a.a0 = static_cast<uint16_t>(x.x);
+  a.a1 = static_cast<uint16_t>(x.x >> 16);
+  a.k0 = static_cast<uint16_t>(x.y);
+  a.k1 = static_cast<uint16_t>(x.y >> 16);
+  a.kmul0 = x.z;
+  a.kmul1 = x.w;
+  a.bias = y.x;
+  a.total = static_cast<int>(y.y);
+  a.soff = static_cast<int>(y.z);
+  a.flags = static_cast<int>(y.w);
+  return a;
 }
 
 // Add one (row, query) match: `get(code)` reads a field of the row.
 template <class Get>
-__device__ __forceinline__ void batch_match(const BQ& Q, int qi, Get get, unsigned long long* s_acc,
-                                            unsigned char* smem, bool& bad_group) {
-  const unsigned long long w = batch_value(Q, get(Q.af[0]), Q.agg_op != MB_AGG_SUM ? get(Q.af[1]) : 0);
-  if (Q.res_layout == MB_RES_SCALAR) {
-    atomicAdd(&s_acc[qi], w);
-    return;
-  }
-  unsigned hh = 0;
-  int k0 = 0, k1 = 0;
-  if (Q.nk > 0) {
-    k0 = get(Q.kf[0]);
-    hh += (static_cast<unsigned>(k0) - static_cast<unsigned>(Q.kmin[0])) * static_cast<unsigned>(Q.kmul[0]);
-  }
-  if (Q.nk > 1) {
-    k1 = get(Q.kf[1]);
-    hh += (static_cast<unsigned>(k1) - static_cast<unsigned>(Q.kmin[1])) * static_cast<unsigned>(Q.kmul[1]);
-  }
+__device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int qi, Get get, unsigned char* smem,
+                                            bool& bad_group) {
+  const unsigned v0 = static_cast<unsigned>(get(A.a0)), v1 = static_cast<unsigned>(get(A.a1));
+  const int op = A.flags & 3;
+  const unsigned u = op == MB_AGG_SUM ? v0 : op == MB_AGG_SUB ? v0 - v1 : v0 * v1;
+  const unsigned long long w = static_cast<unsigned long long>(static_cast<long long>(static_cast<int>(u)));
+  const int k0 = get(A.k0), k1 = get(A.k1);
+  const unsigned hh = static_cast<unsigned>(k0) * A.kmul0 + static_cast<unsigned>(k1) * A.kmul1 + A.bias;
   int g = static_cast<int>(hh);
-  if (static_cast<unsigned>(g) >= static_cast<unsigned>(Q.total_val)) g = g % Q.total_val;
-  if (g < 0) {
-    bad_group = true;
-    return;
-  }
-  int* res = static_cast<int*>(Q.res);
-  if (Q.smem_off >= 0) {
-    // per-CTA partial; the first row of a group in this CTA writes the group's keys
-    unsigned long long* s_sum = reinterpret_cast<unsigned long long*>(smem + Q.smem_off);
-    uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + Q.smem_off + 8 * Q.total_val);
-    atomicAdd(&s_sum[g], w);
-    const uint32_t bit = 1u << (g & 31);
-    if (!(s_touch[g >> 5] & bit) && !(atomicOr(&s_touch[g >> 5], bit) & bit) && Q.res_layout == MB_RES_CRYSTAL4) {
-      if (Q.nk > 0) res[4 * g] = k0;
-      if (Q.nk > 1) res[4 * g + 1] = k1;
+  if (hh >= static_cast<unsigned>(A.total)) {
+    g %= A.total;
+    if (g < 0) {
+      bad_group = true;
+      return;
     }
-    return;
   }
-  if (Q.res_layout == MB_RES_CRYSTAL4) {
-    if (Q.nk > 0) res[4 * g] = k0;
-    if (Q.nk > 1) res[4 * g + 1] = k1;
+  const bool c4 = (A.flags >> 2) & 1;
+  if (A.soff >= 0) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff) + g, w);
+    if (!c4) return;
+    // the first row of a group in this CTA writes the group's keys
+    uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + A.soff + 8 * A.total);
+    const uint32_t bit = 1u << (g & 31);
+    if ((s_touch[g >> 5] & bit) || (atomicOr(&s_touch[g >> 5], bit) & bit)) return;
+  } else {
+    void* res = s_res[qi];
+    atomicAdd(c4 ? reinterpret_cast<unsigned long long*>(static_cast<int*>(res) + 4 * g + 2)
+                 : static_cast<unsigned long long*>(res) + g,
+              w);
+    if (!c4) return;
   }
-  atomicAdd(batch_sum_ptr(Q, g), w);
+  int* res = static_cast<int*>(s_res[qi]);
+  const int nk = (A.flags >> 3) & 3;
+  if (nk > 0) res[4 * g] = k0;
+  if (nk > 1) res[4 * g + 1] = k1;
 }
 
 // The queries accepting one row: presence mask AND one mask per constrained attribute.
@@ -161,17 +185,24 @@ __device__ __forceinline__ void batch_row_mask(const BatchPlan& P, unsigned pres
                                                const unsigned* s_out, const unsigned char* smem, unsigned (&m)[NWM]) {
 #pragma unroll
   for (int w = 0; w < NWM; ++w) m[w] = s_pres[pres * kMaskWordsMax + w];
-  for (int f = 0; f < P.nfields; ++f) {
-    unsigned any = 0;
 #pragma unroll
-    for (int w = 0; w < NWM; ++w) any |= m[w];
-    if (!any) return;
-    const int v = get(P.f_code[f]) - P.f_min[f];
+  for (int f = 0; f < kMaxPredFields; ++f) {
+    if (f >= P.nfields) break;
+    // with one mask word an empty mask ends the row early; with more, rows nearly always
+    // keep some query and the test would cost more than it saves
+    if (NWM == 1 && m[0] == 0) return;
+    const int v = get(P.f_scode[f]) - P.f_min[f];
     const unsigned* t;
-    if (static_cast<unsigned>(v) < static_cast<unsigned>(P.f_n[f]))
-      t = P.f_smem_off[f] >= 0 ? reinterpret_cast<const unsigned*>(smem + P.f_smem_off[f]) + v * P.nwords
-                               : P.tables + P.f_goff[f] + static_cast<long long>(v) * P.nwords;
-    else
+    if (static_cast<unsigned>(v) < static_cast<unsigned>(P.f_n[f])) {
+      int e = v;
+      if (P.f_nint[f] > 0) {
+        const int* bp = reinterpret_cast<const int*>(smem + P.f_bps_off[f]);
+        e = reinterpret_cast<const uint16_t*>(smem + P.f_bkt_off[f])[v >> P.f_shift[f]];
+        while (e + 1 < P.f_nint[f] && bp[e + 1] <= v) ++e;
+      }
+      t = P.f_smem_off[f] >= 0 ? reinterpret_cast<const unsigned*>(smem + P.f_smem_off[f]) + e * P.nwords
+                               : P.tables + P.f_goff[f] + static_cast<long long>(e) * P.nwords;
+    } else
       t = s_out + f * kMaskWordsMax;
     if (NWM >= 4) {
 #pragma unroll
@@ -189,34 +220,17 @@ __device__ __forceinline__ void batch_row_mask(const BatchPlan& P, unsigned pres
   }
 }
 
-// Every query a row's mask selects, processed by the lane that owns the row.
-template <int NWM, class Get>
-__device__ __forceinline__ void batch_row(const BatchPlan& P, unsigned pres, Get get, const BQ* s_desc,
-                                          const unsigned* s_pres, const unsigned* s_out, unsigned long long* s_acc,
-                                          unsigned char* smem, bool& bad_group) {
-  unsigned m[NWM];
-  batch_row_mask<NWM>(P, pres, get, s_pres, s_out, smem, m);
-#pragma unroll
-  for (int w = 0; w < NWM; ++w) {
-    unsigned bits = m[w];
-    while (bits) {
-      const int qi = w * 32 + __ffs(bits) - 1;
-      bits &= bits - 1;
-      batch_match(s_desc[qi], qi, get, s_acc, smem, bad_group);
-    }
-  }
-}
-
 template <int NCW, int ITEMS, int NWM>
 __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_constant__ BatchPlan P) {
   constexpr int WROWS = 32 * ITEMS;
   constexpr int TILE = NCW * WROWS;
+  constexpr int CS = TILE + kColPad;  // stage column stride (words)
   constexpr int NWARPS = NCW + 1;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kBatchStages;
-  unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem + P.smem_acc_off);
-  BQ* s_desc = reinterpret_cast<BQ*>(smem + P.smem_desc_off);
+  AQ* s_aq = reinterpret_cast<AQ*>(smem + P.smem_aq_off);
+  void** s_res = reinterpret_cast<void**>(smem + P.smem_res_off);
   unsigned* s_pres = reinterpret_cast<unsigned*>(smem + P.smem_pres_off);
   unsigned* s_out = reinterpret_cast<unsigned*>(smem + P.smem_out_off);
   int* stage_base = reinterpret_cast<int*>(smem + P.smem_stage_off);
@@ -224,11 +238,14 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
   const int S = P.stages;
 
   // ---- set-up: accumulators, descriptors, masks, small tables, barriers ------------
-  for (int q = tid; q < P.nq; q += NWARPS * 32) s_acc[q] = 0;
   {
-    const unsigned* src = reinterpret_cast<const unsigned*>(P.q);
-    unsigned* dst = reinterpret_cast<unsigned*>(s_desc);
-    for (int w = tid; w < P.nq * static_cast<int>(sizeof(BQ) / 4); w += NWARPS * 32) dst[w] = src[w];
+    unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem + P.smem_acc_off);
+    for (int q = tid; q < P.nq; q += NWARPS * 32) {
+      s_acc[q] = 0;
+      s_res[q] = P.q[q].res;
+    }
+    unsigned* dst = reinterpret_cast<unsigned*>(s_aq);
+    for (int w = tid; w < P.nq * 8; w += NWARPS * 32) dst[w] = reinterpret_cast<const unsigned*>(&P.q[w >> 3].a)[w & 7];
     for (int w = tid; w < 16 * kMaskWordsMax; w += NWARPS * 32) s_pres[w] = (&P.pres_mask[0][0])[w];
     for (int w = tid; w < kMaxPredFields * kMaskWordsMax; w += NWARPS * 32) s_out[w] = (&P.outside[0][0])[w];
     unsigned* g = reinterpret_cast<unsigned*>(smem + P.smem_groups_off);
@@ -237,7 +254,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
       if (P.f_smem_off[f] < 0) continue;
       unsigned* t = reinterpret_cast<unsigned*>(smem + P.f_smem_off[f]);
       const unsigned* s = P.tables + P.f_goff[f];
-      for (int w = tid; w < P.f_n[f] * P.nwords; w += NWARPS * 32) t[w] = s[w];
+      for (int w = tid; w < P.f_ent[f] * P.nwords; w += NWARPS * 32) t[w] = s[w];
+      if (P.f_nint[f] > 0) {
+        int* bp = reinterpret_cast<int*>(smem + P.f_bps_off[f]);
+        for (int i = tid; i < P.f_nint[f]; i += NWARPS * 32) bp[i] = P.bp[P.f_bp_off[f] + i];
+      }
     }
   }
   if (tid == 0) {
@@ -246,6 +267,26 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
       mbar_init(&empty[s], NCW);
     }
     mbar_fence_init();
+  }
+  __syncthreads();
+  // bucket indexes of the interval-coded attributes: the interval of each bucket's first value
+  for (int f = 0; f < P.nfields; ++f) {
+    if (P.f_nint[f] == 0) continue;
+    const int* bp = reinterpret_cast<const int*>(smem + P.f_bps_off[f]);
+    uint16_t* bkt = reinterpret_cast<uint16_t*>(smem + P.f_bkt_off[f]);
+    const int nb = ((P.f_n[f] - 1) >> P.f_shift[f]) + 1;
+    for (int b = tid; b < nb; b += NWARPS * 32) {
+      const int v0 = b << P.f_shift[f];
+      int lo = 0, hi = P.f_nint[f] - 1;  // bp[0] = 0 <= v0: find the last bp[i] <= v0
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bp[mid] <= v0)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      bkt[b] = static_cast<uint16_t>(lo);
+    }
   }
   __syncthreads();
 
@@ -268,7 +309,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         int* dst = stage_base + s * P.stage_words;
         fence_proxy_async_smem();
         mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>(P.ncols) * TILE * 4u);
-        for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, &full[s], policy);
+        for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * CS, P.col[c] + r0, TILE * 4, &full[s], policy);
         if (++s == S) {
           s = 0;
           phase ^= 1u;
@@ -279,6 +320,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
     }
   } else {
     const int cw = warp - 1;
+    unsigned* mlist = reinterpret_cast<unsigned*>(smem + P.smem_list_off) + cw * P.list_cap;
     int s = 0;
     uint32_t phase = 0;
     for (long long k = 0; k < my_tiles; ++k) {
@@ -291,40 +333,47 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
       // ---- dimension words, once per row for the whole batch -------------------
       for (int t = 0; t < P.ndims; ++t) {
         const int d = P.dim_list[t];
-        const int* kcol = wst + P.key_stage[d] * TILE;
-        int* out = wst + P.cidx[MB_COL_DIM_S + d] * TILE;
+        const int* kcol = wst + P.key_stage[d] * CS;
+        int* out = wst + P.cidx[MB_COL_DIM_S + d] * CS;
         const unsigned* pat = P.pat[d];
         const int slots = P.pat_slots[d], kmin = P.pat_kmin[d];
         unsigned wv[ITEMS];
-#pragma unroll
-        for (int j = 0; j < ITEMS / 4; ++j) {
-          const int4 kv = lds128(kcol + (j * 32 + lane) * 4);
-          const int keys[4] = {kv.x, kv.y, kv.z, kv.w};
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int h = bslot(keys[e], slots, kmin);
-            if (h < 0) {
-              bad_probe = true;
-              wv[4 * j + e] = 0;
-            } else {
-              wv[4 * j + e] = __ldg(pat + h);
-            }
+        auto lookup = [&](int key) -> unsigned {
+          const int h = bslot(key, slots, kmin);
+          if (h < 0) {
+            bad_probe = true;
+            return 0u;
           }
-        }
+          return __ldg(pat + h);
+        };
+        if constexpr (ITEMS % 4 == 0) {
 #pragma unroll
-        for (int j = 0; j < ITEMS / 4; ++j) {
-          int4 o;
-          o.x = static_cast<int>(wv[4 * j]);
-          o.y = static_cast<int>(wv[4 * j + 1]);
-          o.z = static_cast<int>(wv[4 * j + 2]);
-          o.w = static_cast<int>(wv[4 * j + 3]);
-          *reinterpret_cast<int4*>(out + (j * 32 + lane) * 4) = o;
+          for (int j = 0; j < ITEMS / 4; ++j) {
+            const int4 kv = lds128(kcol + (j * 32 + lane) * 4);
+            wv[4 * j] = lookup(kv.x);
+            wv[4 * j + 1] = lookup(kv.y);
+            wv[4 * j + 2] = lookup(kv.z);
+            wv[4 * j + 3] = lookup(kv.w);
+          }
+#pragma unroll
+          for (int j = 0; j < ITEMS / 4; ++j) {
+            int4 o;
+            o.x = static_cast<int>(wv[4 * j]);
+            o.y = static_cast<int>(wv[4 * j + 1]);
+            o.z = static_cast<int>(wv[4 * j + 2]);
+            o.w = static_cast<int>(wv[4 * j + 3]);
+            *reinterpret_cast<int4*>(out + (j * 32 + lane) * 4) = o;
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < ITEMS; ++e) wv[e] = lookup(kcol[e * 32 + lane]);
+#pragma unroll
+          for (int e = 0; e < ITEMS; ++e) out[e * 32 + lane] = static_cast<int>(wv[e]);
         }
       }
       __syncwarp();
-      // ---- query masks row by row; matches go through the warp's list so that every
-      // lane aggregates one (row, query) pair at a time -----------------------------
-      unsigned* mlist = reinterpret_cast<unsigned*>(smem + P.smem_list_off) + cw * kMatchListCap;
+      // ---- query masks row by row (lane l takes rows l, 32 + l, ...); matches go
+      // through the warp's list so that every lane aggregates one pair at a time ------
       int lpos = 0;
       auto flush = [&](int n) {
         for (int base = 0; base < n; base += 32) {
@@ -332,21 +381,21 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
           if (idx < n) {
             const unsigned pr = mlist[idx];
             const int row = static_cast<int>(pr >> 16), qi = static_cast<int>(pr & 0xffffu);
-            auto get = [&](int code) { return field_value(wst[P.cidx[code >> 11] * TILE + row], code); };
-            batch_match(s_desc[qi], qi, get, s_acc, smem, bad_group);
+            auto get = [&](int code) { return field_value(wst[(code >> 11) * CS + row], code); };
+            batch_match(load_aq(s_aq, qi), s_res, qi, get, smem, bad_group);
           }
         }
         __syncwarp();
       };
 #pragma unroll 1
       for (int i = 0; i < ITEMS; ++i) {
-        const int row = ((i >> 2) * 32 + lane) * 4 + (i & 3);
+        const int row = i * 32 + lane;
         unsigned pres = 0;
         for (int t = 0; t < P.ndims; ++t) {
           const int d = P.dim_list[t];
-          pres |= (static_cast<unsigned>(wst[P.cidx[MB_COL_DIM_S + d] * TILE + row]) >> 31) << d;
+          pres |= (static_cast<unsigned>(wst[P.cidx[MB_COL_DIM_S + d] * CS + row]) >> 31) << d;
         }
-        auto get = [&](int code) { return field_value(wst[P.cidx[code >> 11] * TILE + row], code); };
+        auto get = [&](int code) { return field_value(wst[(code >> 11) * CS + row], code); };
         unsigned m[NWM];
         batch_row_mask<NWM>(P, pres, get, s_pres, s_out, smem, m);
         int cnt = 0;
@@ -360,11 +409,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         }
         const int total = __shfl_sync(kFullMask, incl, 31);
         if (total == 0) continue;
-        if (lpos + total > kMatchListCap) {
+        if (lpos + total > P.list_cap) {
           flush(lpos);
           lpos = 0;
         }
-        if (total > kMatchListCap) {
+        if (total > P.list_cap) {
           // more matches than the list holds: this row runs lane by lane
 #pragma unroll
           for (int w = 0; w < NWM; ++w) {
@@ -372,7 +421,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
             while (bits) {
               const int qi = w * 32 + __ffs(bits) - 1;
               bits &= bits - 1;
-              batch_match(s_desc[qi], qi, get, s_acc, smem, bad_group);
+              batch_match(load_aq(s_aq, qi), s_res, qi, get, smem, bad_group);
             }
           }
           __syncwarp();
@@ -406,8 +455,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         uint32_t pr = 0;
         for (int t = 0; t < P.ndims; ++t) {
           const int d = P.dim_list[t];
-          const int key_col = d == 0 ? MB_COL_SUPPKEY : d == 1 ? MB_COL_CUSTKEY : d == 2 ? MB_COL_PARTKEY : MB_COL_ORDERDATE;
-          const int h = bslot(__ldg(P.fact_all[key_col] + r), P.pat_slots[d], P.pat_kmin[d]);
+          const int h = bslot(__ldg(P.col[P.key_stage[d]] + r), P.pat_slots[d], P.pat_kmin[d]);
           if (h < 0) {
             bad_probe = true;
             continue;
@@ -417,9 +465,20 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         }
         auto get = [&](int code) {
           const int c = code >> 11;
-          return field_value(c >= MB_COL_DIM_S ? dimw[c - MB_COL_DIM_S] : __ldg(P.fact_all[c] + r), code);
+          const int d = P.stage_dim[c];
+          return field_value(d >= 0 ? dimw[d] : __ldg(P.col[c] + r), code);
         };
-        batch_row<NWM>(P, pr, get, s_desc, s_pres, s_out, s_acc, smem, bad_group);
+        unsigned m[NWM];
+        batch_row_mask<NWM>(P, pr, get, s_pres, s_out, smem, m);
+#pragma unroll
+        for (int w = 0; w < NWM; ++w) {
+          unsigned bits = m[w];
+          while (bits) {
+            const int qi = w * 32 + __ffs(bits) - 1;
+            bits &= bits - 1;
+            batch_match(load_aq(s_aq, qi), s_res, qi, get, smem, bad_group);
+          }
+        }
       }
     }
   }
@@ -428,16 +487,20 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
   if (bad_probe) set_status(P.status, MB_STATUS_PROBE_RANGE);
   if (bad_group) set_status(P.status, MB_STATUS_GROUP_RANGE);
   __syncthreads();
-  for (int q = tid; q < P.nq; q += NWARPS * 32)
-    if (s_desc[q].res_layout == MB_RES_SCALAR && s_acc[q] != 0)
-      atomicAdd(static_cast<unsigned long long*>(s_desc[q].res), s_acc[q]);
+  // ---- fold this CTA's scalars and shared-memory group arrays into the results -------
+  // (a zero partial is skipped: adding it changes nothing)
   for (int q = 0; q < P.nq; ++q) {
-    const BQ& Q = s_desc[q];
-    if (Q.smem_off < 0) continue;
-    const unsigned long long* s_sum = reinterpret_cast<const unsigned long long*>(smem + Q.smem_off);
-    const uint32_t* s_touch = reinterpret_cast<const uint32_t*>(smem + Q.smem_off + 8 * Q.total_val);
-    for (int g = tid; g < Q.total_val; g += NWARPS * 32)
-      if ((s_touch[g >> 5] >> (g & 31)) & 1u) atomicAdd(batch_sum_ptr(Q, g), s_sum[g]);
+    const AQ A = s_aq[q];
+    if (A.soff < 0) continue;
+    const unsigned long long* s_sum = reinterpret_cast<const unsigned long long*>(smem + A.soff);
+    const bool c4 = (A.flags >> 2) & 1;
+    for (int g = tid; g < A.total; g += NWARPS * 32) {
+      const unsigned long long v = s_sum[g];
+      if (v == 0) continue;
+      atomicAdd(c4 ? reinterpret_cast<unsigned long long*>(static_cast<int*>(s_res[q]) + 4 * g + 2)
+                   : static_cast<unsigned long long*>(s_res[q]) + g,
+                v);
+    }
   }
 }
 
@@ -450,8 +513,9 @@ __global__ void batch_mask_kernel(const __grid_constant__ BatchPlan P) {
     const int w = static_cast<int>(e % P.nwords);
     long long v = e / P.nwords;
     int f = 0;
-    while (f < P.nfields - 1 && v >= P.f_n[f]) v -= P.f_n[f++];
-    const int x = P.f_min[f] + static_cast<int>(v);
+    while (f < P.nfields - 1 && v >= P.f_ent[f]) v -= P.f_ent[f++];
+    // an interval's verdicts are those of its first value
+    const int x = P.f_min[f] + (P.f_nint[f] > 0 ? P.bp[P.f_bp_off[f] + v] : static_cast<int>(v));
     const int code = P.f_code[f];
     unsigned bits = 0;
     for (int j = 0; j < 32; ++j) {
@@ -505,8 +569,11 @@ struct BatchVariant {
 #define MB_BATCH_VARIANTS(W, I) \
   {W, I, 1, batch_kernel<W, I, 1>}, {W, I, 2, batch_kernel<W, I, 2>}, {W, I, 4, batch_kernel<W, I, 4>}, \
       {W, I, 8, batch_kernel<W, I, 8>}
+// (consumer warps, rows per lane per stage): more warps per CTA hide more latency; fewer
+// rows per lane keep their stage ring small enough for that
 static const BatchVariant kBatchVariants[] = {
-    MB_BATCH_VARIANTS(4, 4), MB_BATCH_VARIANTS(8, 4), MB_BATCH_VARIANTS(16, 4), MB_BATCH_VARIANTS(8, 8),
+    MB_BATCH_VARIANTS(8, 4), MB_BATCH_VARIANTS(16, 4), MB_BATCH_VARIANTS(16, 2),
+    MB_BATCH_VARIANTS(24, 1), MB_BATCH_VARIANTS(24, 2), MB_BATCH_VARIANTS(30, 1),
 };
 
 static bool field_ok(int code) {
@@ -547,6 +614,8 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
     }
     return true;
   };
+  // row-schema codes of the aggregation fields, converted to stage codes below
+  int af[MB_BATCH_MAX_QUERIES][2], kf[MB_BATCH_MAX_QUERIES][2];
   for (int qi = 0; qi < P.nq; ++qi) {
     const mb_batch_query& q = a->queries[qi];
     BQ& d = P.q[qi];
@@ -557,12 +626,9 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
     if (q.res_layout != MB_RES_SCALAR && q.total_val <= 0) return MB_ERR_ARG;
     if (!aligned8(q.res)) return MB_ERR_ALIGN;
     if (q.dims_required < 0 || q.dims_required > 15) return MB_ERR_ARG;
+    const int nk = q.res_layout == MB_RES_SCALAR ? 0 : q.num_keys;
     d.np = static_cast<uint8_t>(q.num_preds);
-    d.nk = static_cast<uint8_t>(q.res_layout == MB_RES_SCALAR ? 0 : q.num_keys);
-    d.agg_op = static_cast<uint8_t>(q.agg_op);
     d.res_layout = static_cast<uint8_t>(q.res_layout);
-    d.req = static_cast<uint8_t>(q.dims_required);
-    d.smem_off = -1;
     dims_used |= static_cast<unsigned>(q.dims_required);
     for (int p = 0; p < q.num_preds; ++p) {
       if (!note_field(q.pred_field[p])) return MB_ERR_ARG;
@@ -570,17 +636,23 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
       d.plo[p] = q.pred_lo[p];
       d.phi[p] = q.pred_hi[p];
     }
-    for (int k = 0; k < (q.agg_op == MB_AGG_SUM ? 1 : 2); ++k) {
+    for (int k = 0; k < (q.agg_op == MB_AGG_SUM ? 1 : 2); ++k)
       if (!note_field(q.agg_field[k])) return MB_ERR_ARG;
-      d.af[k] = static_cast<uint16_t>(q.agg_field[k]);
-    }
-    for (int k = 0; k < d.nk; ++k) {
+    af[qi][0] = q.agg_field[0];
+    af[qi][1] = q.agg_op == MB_AGG_SUM ? q.agg_field[0] : q.agg_field[1];
+    for (int k = 0; k < nk; ++k)
       if (!note_field(q.key_field[k])) return MB_ERR_ARG;
-      d.kf[k] = static_cast<uint16_t>(q.key_field[k]);
-      d.kmin[k] = q.key_min[k];
-      d.kmul[k] = q.key_mul[k];
-    }
-    d.total_val = q.res_layout == MB_RES_SCALAR ? 1 : q.total_val;
+    // an absent key reads the first aggregation field and weighs it by 0
+    kf[qi][0] = nk > 0 ? q.key_field[0] : af[qi][0];
+    kf[qi][1] = nk > 1 ? q.key_field[1] : af[qi][0];
+    AQ& A = d.a;
+    A.kmul0 = nk > 0 ? static_cast<unsigned>(q.key_mul[0]) : 0u;
+    A.kmul1 = nk > 1 ? static_cast<unsigned>(q.key_mul[1]) : 0u;
+    A.bias = 0u - ((nk > 0 ? static_cast<unsigned>(q.key_min[0]) * A.kmul0 : 0u) +
+                   (nk > 1 ? static_cast<unsigned>(q.key_min[1]) * A.kmul1 : 0u));
+    A.total = q.res_layout == MB_RES_SCALAR ? 1 : q.total_val;
+    A.soff = -1;
+    A.flags = q.agg_op | ((q.res_layout == MB_RES_CRYSTAL4 ? 1 : 0) << 2) | (nk << 3);
     d.res = q.res;
   }
   // constrained attributes and the hull of the ranges on each
@@ -607,13 +679,43 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
     }
   }
   long long entries = 0;
+  int nbp = 0;
   for (int f = 0; f < P.nfields; ++f) {
     const long long n = has[f] ? static_cast<long long>(hmax[f]) - hmin[f] + 1 : 1;
     if (n > 65536) return MB_ERR_SIZE;  // attribute ranges wider than 65,536 values
     P.f_min[f] = has[f] ? hmin[f] : 0;
     P.f_n[f] = static_cast<int>(n);
+    P.f_ent[f] = P.f_n[f];
+    if (n > kSmemTableMaxEntries) {
+      // interval coding: end points lo and hi + 1 of every non-empty range on f, and 0
+      int pts[2 * MB_BATCH_MAX_QUERIES * MB_BATCH_MAX_PREDS + 1];
+      int np = 0;
+      pts[np++] = 0;
+      for (int qi = 0; qi < P.nq; ++qi) {
+        const BQ& d = P.q[qi];
+        for (int p = 0; p < d.np; ++p) {
+          if (d.pf[p] != P.f_code[f] || d.plo[p] > d.phi[p]) continue;
+          const long long lo = static_cast<long long>(d.plo[p]) - P.f_min[f];
+          const long long hi1 = static_cast<long long>(d.phi[p]) + 1 - P.f_min[f];
+          if (lo > 0) pts[np++] = static_cast<int>(lo);
+          if (hi1 < n) pts[np++] = static_cast<int>(hi1);
+        }
+      }
+      std::sort(pts, pts + np);
+      np = static_cast<int>(std::unique(pts, pts + np) - pts);
+      if (nbp + np <= kMaxBreakpoints) {
+        P.f_nint[f] = np;
+        P.f_bp_off[f] = nbp;
+        for (int i = 0; i < np; ++i) P.bp[nbp + i] = pts[i];
+        nbp += np;
+        int shift = 0;
+        while ((static_cast<long long>(kMaxBuckets) << shift) < n) ++shift;
+        P.f_shift[f] = shift;
+        P.f_ent[f] = np;
+      }
+    }
     P.f_goff[f] = entries * P.nwords;
-    entries += P.f_n[f];
+    entries += P.f_ent[f];
   }
   P.table_entries = entries;
   // values outside a hull fail every query constraining that attribute
@@ -624,8 +726,10 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
       if (!constrains) P.outside[f][qi / 32] |= 1u << (qi % 32);
     }
   for (int pm = 0; pm < 16; ++pm)
-    for (int qi = 0; qi < P.nq; ++qi)
-      if ((pm & P.q[qi].req) == P.q[qi].req) P.pres_mask[pm][qi / 32] |= 1u << (qi % 32);
+    for (int qi = 0; qi < P.nq; ++qi) {
+      const unsigned req = static_cast<unsigned>(a->queries[qi].dims_required);
+      if ((pm & req) == req) P.pres_mask[pm][qi / 32] |= 1u << (qi % 32);
+    }
 
   // dimensions: their keys are staged, their words overwrite the key columns (the date
   // word gets its own column because orderdate is also a field)
@@ -636,6 +740,7 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
     fact_used[kKeyCol[d]] = true;
   }
   for (int c = 0; c < 13; ++c) P.cidx[c] = -1;
+  for (int c = 0; c < kMaxStageCols; ++c) P.stage_dim[c] = -1;
   for (int c = 0; c < MB_NUM_FACT_COLS; ++c) {
     P.fact_all[c] = a->fact[c];
     if (!fact_used[c]) continue;
@@ -651,22 +756,31 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
     P.pat_slots[d] = a->dim[d].slots;
     P.pat_kmin[d] = a->dim[d].key_min;
     P.cidx[MB_COL_DIM_S + d] = d == 3 ? P.ncols : P.key_stage[d];
+    P.stage_dim[P.cidx[MB_COL_DIM_S + d]] = d;
   }
   // a dimension word that replaces its key makes that key unavailable as a field
+  auto uses_key = [&](int code) {
+    const int col = code >> 11;
+    for (int t = 0; t < 3; ++t)
+      if ((dims_used & (1u << t)) && col == kKeyCol[t]) return true;
+    return false;
+  };
   for (int qi = 0; qi < P.nq; ++qi) {
     const BQ& d = P.q[qi];
-    auto uses_key = [&](int code) {
-      const int col = code >> 11;
-      for (int t = 0; t < 3; ++t)
-        if ((dims_used & (1u << t)) && col == kKeyCol[t]) return true;
-      return false;
-    };
     for (int p = 0; p < d.np; ++p)
       if (uses_key(d.pf[p])) return MB_ERR_ARG;
-    for (int k = 0; k < (d.agg_op == MB_AGG_SUM ? 1 : 2); ++k)
-      if (uses_key(d.af[k])) return MB_ERR_ARG;
-    for (int k = 0; k < d.nk; ++k)
-      if (uses_key(d.kf[k])) return MB_ERR_ARG;
+    for (int k = 0; k < 2; ++k)
+      if (uses_key(af[qi][k]) || uses_key(kf[qi][k])) return MB_ERR_ARG;
+  }
+  // stage codes
+  auto scode = [&](int code) { return (P.cidx[code >> 11] << 11) | (code & 0x7ff); };
+  for (int f = 0; f < P.nfields; ++f) P.f_scode[f] = scode(P.f_code[f]);
+  for (int qi = 0; qi < P.nq; ++qi) {
+    AQ& A = P.q[qi].a;
+    A.a0 = static_cast<uint16_t>(scode(af[qi][0]));
+    A.a1 = static_cast<uint16_t>(scode(af[qi][1]));
+    A.k0 = static_cast<uint16_t>(scode(kf[qi][0]));
+    A.k1 = static_cast<uint16_t>(scode(kf[qi][1]));
   }
   return MB_OK;
 }
@@ -723,8 +837,9 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   if (ds == nullptr) return err;
   P.status = ds->status;
 
-  const int threads = a->threads ? a->threads : 256;
-  const int items = a->items_per_thread ? a->items_per_thread : 4;
+  // defaults measured best for 256 queries over 120M rows: 24 consumer warps, one row a lane
+  const int threads = a->threads ? a->threads : 768;
+  const int items = a->items_per_thread ? a->items_per_thread : 1;
   const int nwm = P.nwords;
   const BatchVariant* var = nullptr;
   for (const BatchVariant& v : kBatchVariants)
@@ -732,49 +847,65 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   if (var == nullptr) return MB_ERR_ARG;
   const int tile = threads * items;
   P.nfull = P.n / tile;
-  P.stage_words = (P.ncols + ((P.ndims && P.dim_list[P.ndims - 1] == 3) ? 1 : 0)) * tile;
+  P.stage_words = (P.ncols + ((P.ndims && P.dim_list[P.ndims - 1] == 3) ? 1 : 0)) * (tile + kColPad);
   int stages = a->stages ? a->stages : 2;
   if (stages < 2 || stages > kBatchStages) return MB_ERR_ARG;
 
-  // shared memory: barriers | scalars | descriptors | presence masks | outside masks |
-  // small predicate tables | small group arrays | stage ring
+  // shared memory: barriers | scalars | aggregation descriptors | result pointers |
+  // presence masks | outside masks | small predicate tables | match lists |
+  // small group arrays | stage ring
   int off = 2 * kBatchStages * 8;
   P.smem_acc_off = off;
   off += 8 * P.nq;
   off = (off + 15) / 16 * 16;
-  P.smem_desc_off = off;
-  off += static_cast<int>(sizeof(BQ)) * P.nq;
+  P.smem_aq_off = off;
+  off += static_cast<int>(sizeof(AQ)) * P.nq;
+  P.smem_res_off = off;
+  off += 8 * P.nq;
   off = (off + 15) / 16 * 16;
   P.smem_pres_off = off;
   off += 16 * kMaskWordsMax * 4;
   P.smem_out_off = off;
   off += kMaxPredFields * kMaskWordsMax * 4;
-  P.smem_tab_off = off;
   for (int f = 0; f < P.nfields; ++f) {
     P.f_smem_off[f] = -1;
-    if (P.f_n[f] <= kSmemTableMaxEntries) {
+    if (P.f_ent[f] <= kSmemTableMaxEntries || P.f_nint[f] > 0) {
       P.f_smem_off[f] = off;
-      off += (P.f_n[f] * P.nwords * 4 + 15) / 16 * 16;
+      off += (P.f_ent[f] * P.nwords * 4 + 15) / 16 * 16;
+    }
+    if (P.f_nint[f] > 0) {
+      P.f_bps_off[f] = off;
+      off += (P.f_nint[f] * 4 + 15) / 16 * 16;
+      P.f_bkt_off[f] = off;
+      off += ((((P.f_n[f] - 1) >> P.f_shift[f]) + 1) * 2 + 15) / 16 * 16;
     }
   }
   P.smem_list_off = off;
-  off += (threads / 32) * kMatchListCap * 4;
   const int budget = ds->max_smem_optin - 2048;
   auto total_smem = [&](int base, int st) { return (base + 127) / 128 * 128 + st * P.stage_words * 4; };
+  // match lists: 1,024 pairs a warp, or 512 where that leaves shared-memory group arrays
+  // less than 64 KB (a list must hold the pairs of 32 rows with ease: ~8 queries a row
+  // pass on average in a batch of 256 with log-uniform selectivities up to 0.3)
+  P.list_cap = kMatchListMax;
+  if (total_smem(off + (threads / 32) * P.list_cap * 4, stages) > budget - 65536) P.list_cap = 512;
+  off += (threads / 32) * P.list_cap * 4;
   while (total_smem(off, stages) > budget && stages > 2) --stages;
   if (total_smem(off, stages) > budget) return MB_ERR_SIZE;
   P.stages = stages;
+  // scalars accumulate in their shared-memory word
+  for (int qi = 0; qi < P.nq; ++qi)
+    if (P.q[qi].res_layout == MB_RES_SCALAR) P.q[qi].a.soff = P.smem_acc_off + 8 * qi;
   // small group arrays (<= 1,024 groups) to shared memory, smallest first, within the budget
   P.smem_groups_off = off;
   int groups_bytes = 0;
-  const int group_cap = a->smem_group_bytes < 0 ? 65536 : a->smem_group_bytes;
+  const int group_cap = a->smem_group_bytes < 0 ? 131072 : a->smem_group_bytes;
   for (int pass_total = 1; pass_total <= 1024; pass_total *= 2) {
     for (int qi = 0; qi < P.nq; ++qi) {
-      BQ& d = P.q[qi];
-      if (d.res_layout == MB_RES_SCALAR || d.smem_off >= 0 || d.total_val > pass_total) continue;
-      const int bytes = (8 * d.total_val + 4 * ((d.total_val + 31) / 32) + 15) / 16 * 16;
+      AQ& A = P.q[qi].a;
+      if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total > pass_total) continue;
+      const int bytes = (8 * A.total + 4 * ((A.total + 31) / 32) + 15) / 16 * 16;
       if (groups_bytes + bytes > group_cap || total_smem(off + groups_bytes + bytes, stages) > budget) continue;
-      d.smem_off = off + groups_bytes;
+      A.soff = off + groups_bytes;
       groups_bytes += bytes;
     }
   }

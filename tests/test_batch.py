@@ -64,9 +64,9 @@ def test_batch_launch_configs_and_oracle():
     qs = B.generate_queries(24, seed=3, sel_lo=1e-3, sel_hi=0.5)
     base = [q.result_buffer() for q in qs]
     B.run_batch(t, pats, qs, base, n)
-    for threads in (128, 256, 512):
-        for items in (4, 8):
-            for stages in (2, 3):
+    for threads, items in ((256, 4), (512, 4), (512, 2), (768, 1), (768, 2), (960, 1), (128, 4)):
+        for stages in (2, 3):
+            if True:
                 res = [q.result_buffer() for q in qs]
                 try:
                     B.run_batch(t, pats, qs, res, n, threads=threads, items=items, stages=stages)
@@ -99,4 +99,44 @@ def test_batch_launch_configs_and_oracle():
                             layout=1, min_val=1992, unique_val=1, res_slot=0)],
                aggr=[h["lo_revenue"], h["lo_supplycost"]], agg_op=1, total_val=ssb.QB_GROUPS, res_layout=2, res=exp)
         assert np.array_equal(r.cpu().numpy(), exp)
+    assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
+def test_batch_wide_attributes_interval_and_table_paths():
+    """Two wide attributes (orderdate over its calendar, extendedprice over a 60,000-value
+    window) with 256 queries: more range end points than the interval coding takes, so
+    one attribute is interval-coded and the other uses the full value table. Every
+    filter-aggregate result is checked against numpy."""
+    import torch
+    from mordred_b200 import _lib as L
+    torch.cuda.set_device(0)
+    n = 2_000_003
+    s = ssb.Sizes(lo_len=n, s_len=2_000, c_len=30_000, p_len=20_000)
+    t = ssb.gen_device(s, 17, B.BATCH_FACT, B.BATCH_DIMS)
+    pats = B.build_pats(t, s)
+    rng = np.random.default_rng(5)
+    qs = B.generate_queries(256, seed=21, sel_lo=0.05, sel_hi=0.3, templates=("agg",))
+    for q in qs:
+        lo = 1_000_000 + int(rng.integers(0, 30_000))
+        q.extra = [(B.FACT["lo_extendedprice"], lo, lo + int(rng.integers(1, 30_000)))]
+    # both attributes need more end points together than the interval coding takes (768)
+    def points(ranges):
+        lo0, hi0 = min(r[0] for r in ranges), max(r[1] for r in ranges)
+        return len({0} | {r[0] - lo0 for r in ranges if r[0] > lo0} | {r[1] + 1 - lo0 for r in ranges if r[1] < hi0})
+    assert points([q.date for q in qs]) + points([q.extra[0][1:] for q in qs]) > 768
+    res = [q.result_buffer() for q in qs]
+    B.run_batch(t, pats, qs, res, n)
+    h = {k: t[k].cpu().numpy().astype(np.int64) for k in ("lo_orderdate", "lo_discount", "lo_quantity",
+                                                          "lo_extendedprice")}
+    nonzero = 0
+    for q, r in zip(qs, res):
+        m = ((h["lo_orderdate"] >= q.date[0]) & (h["lo_orderdate"] <= q.date[1])
+             & (h["lo_discount"] >= q.discount[0]) & (h["lo_discount"] <= q.discount[1])
+             & (h["lo_quantity"] >= q.quantity[0]) & (h["lo_quantity"] <= q.quantity[1])
+             & (h["lo_extendedprice"] >= q.extra[0][1]) & (h["lo_extendedprice"] <= q.extra[0][2]))
+        exp = int((h["lo_extendedprice"][m] * h["lo_discount"][m]).sum())
+        assert int(r.item()) == exp
+        nonzero += exp != 0
+    assert nonzero > 200
     assert L.device_status(0) == 0
