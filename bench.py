@@ -8,6 +8,11 @@ configured shapes) and larger than L2, so no flush is needed between steps.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
+Beside the headline the line reports, outside the timed steps: the filter-aggregate
+(16 B/row) on the full table and on its own 6 M-row table with L2 flushed; and a batch
+of 256 generated queries run as one shared scan (CUDA graph replay) against the same
+queries run one at a time, with the results compared bit for bit.
+
 N > 1 runs under torchrun: rank r holds rows [r*120M, (r+1)*120M) of one table
 (weak scaling), and each step all-reduces the dense group sums over NCCL.
 The reference arm (--impl reference) times the reference's own CPU engine
@@ -19,7 +24,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -45,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-sample-rows", type=int, default=24_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-queries", type=int, default=256)
     return ap.parse_args()
 
 
@@ -57,57 +63,69 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clock and throttle reasons of one GPU, polled through NVML every 5 ms while the
+    timed region runs (short enough to sample a region of a few tens of milliseconds)."""
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[int, int]] = []
+        self.max_mhz = None
+        self.error = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _handle(self):
+        import pynvml as N
+        import torch
+
+        N.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.device)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return N.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return N.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _run(self, h):
+        import pynvml as N
+
+        while not self._stop.is_set():
+            try:
+                self.samples.append((N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM),
+                                     N.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception as e:  # keep what was sampled
+                self.error = str(e)
+                return
+            self._stop.wait(0.005)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+            import pynvml as N
+
+            h = self._handle()
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            self._t = threading.Thread(target=self._run, args=(h,), daemon=True)
+            self._t.start()
+        except Exception as e:
+            self.error = str(e)
         return self
 
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
-
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        if self._t is not None:
+            self._t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[3:7]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [c for c, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS.items() if r & bit})
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+               "samples": len(sm), "source": "NVML, 5 ms polling during the timed region"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def cpu_baseline_reference(rows: int, trials: int, threads: int = 0):
@@ -138,6 +156,78 @@ def cpu_baseline_port(rows: int, trials: int):
         O.q41(h, ssb.DATE_SLOTS)
         steps.append((time.perf_counter() - t0) * 1e3)
     return steps, os.cpu_count() or 1
+
+
+def batch_section(t, s, n, rank, world, args):
+    """256 generated queries (filter-aggregate, Query A and Query B forms; selectivities
+    log-uniform in [1e-5, 0.3]) over this rank's fact rows: one batched scan, replayed
+    from a CUDA graph, against running the queries one at a time (filtered builds + the
+    fused probe per query, the reference's way). Results are compared bit for bit."""
+    import torch
+    import torch.distributed as dist
+
+    from mordred_b200 import _lib as L
+    from mordred_b200 import batch as B
+    from mordred_b200 import ssb
+
+    st = ssb._stream()
+    for name in B.BATCH_FACT:
+        if name not in t:
+            buf = torch.empty(n, dtype=torch.int32, device="cuda")
+            L.call("mb_gen_fact_column", ssb.FACT_COLUMNS[name], SEED, rank * n, n, s.s_len, s.c_len, s.p_len,
+                   ssb._p(buf), st)
+            t[name] = buf
+    t.update(ssb.gen_device(s, SEED, [], [d for d in B.BATCH_DIMS if d not in t]))
+    pats = B.build_pats(t, s)
+    qs = B.generate_queries(args.batch_queries, seed=SEED)
+    flat, views = B.result_buffers(qs)
+    plan = B.BatchPlan(t, pats, qs, views, n)
+    graph = plan.capture(zero=flat)
+    for _ in range(3):
+        graph.replay()
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1) / reps
+    ws = B.AloneWorkspace(s)
+    alone = [q.result_buffer() for q in qs]
+
+    def one_at_a_time():
+        for r in alone:
+            r.zero_()
+        for q, r in zip(qs, alone):
+            B.run_alone(t, ws, q, r, n)
+
+    one_at_a_time()
+    torch.cuda.synchronize()
+    a_reps = 2
+    e0.record()
+    for _ in range(a_reps):
+        one_at_a_time()
+    e1.record()
+    torch.cuda.synchronize()
+    alone_ms = e0.elapsed_time(e1) / a_reps
+    equal = all(torch.equal(a.view(-1), b.view(-1)) for a, b in zip(views, alone))
+    tm = torch.tensor([batch_ms, alone_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    batch_ms, alone_ms = float(tm[0]), float(tm[1])
+    del graph
+    cols = len(B.BATCH_FACT)
+    peak, peak_kind = measured_peaks()
+    return {"queries": len(qs), "fact_rows_per_gpu": n, "templates": {k: sum(q.template == k for q in qs)
+                                                                      for k in ("agg", "qa", "qb")},
+            "expected_matches_per_row": sum(q.meta["expected_selectivity"] for q in qs),
+            "batched_ms": batch_ms, "one_at_a_time_ms": alone_ms, "speedup": alone_ms / batch_ms,
+            "query_rows_per_s": len(qs) * n * world / (batch_ms / 1e3),
+            "shared_scan_gbs": cols * 4 * n / batch_ms / 1e6, "shared_scan_frac_of_hbm": cols * 4 * n / batch_ms / 1e6 / peak,
+            "peak_kind": peak_kind, "results_equal_one_at_a_time": equal,
+            "launch": "CUDA graph replay (result memset + mask kernel + batch kernel)", "seed": SEED}
 
 
 def run_reference_arm(args, rank, world):
@@ -196,7 +286,7 @@ def main():
     # rank r holds rows [r*n, (r+1)*n) of one fact table; dimensions are replicated
     t = {}
     st = ssb._stream()
-    for name in ssb.QB_FACT:
+    for name in ssb.QB_FACT + ["lo_discount", "lo_quantity", "lo_extendedprice"]:
         buf = torch.empty(n, dtype=torch.int32, device="cuda")
         L.call("mb_gen_fact_column", ssb.FACT_COLUMNS[name], SEED, rank * n, n, s.s_len, s.c_len, s.p_len,
                ssb._p(buf), st)
@@ -276,6 +366,31 @@ def main():
         if k:
             traffic = k["bytes_per_launch_scaled"]
 
+    # ---- filter-aggregate (16 B/row): the full table, and the 6 M-row table of its own
+    # workload (96 MB, inside L2: a 512 MB write flushes L2 before every timed launch) -------
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def time_q11(rows, reps, do_flush):
+        ms = []
+        for _ in range(reps + 2):
+            if do_flush:
+                flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ssb.q11(t, rows, ws, zero=False)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms[2:])
+
+    f_full = time_q11(n, 20, False)
+    f_small_rows = min(n, 6_000_000)
+    f_small = time_q11(f_small_rows, 20, True)
+    del flush
+
+    # ---- batched multi-query execution: 256 queries over the same fact rows ---------------
+    batched = None if args.no_batch else batch_section(t, s, n, rank, world, args)
+
     # ---- end to end: host-resident tables through the public API ---------------------------
     e2e = None
     if not args.no_e2e:
@@ -332,6 +447,13 @@ def main():
                        "l2": "inputs larger than L2 (1.92 GB + 2.88 GB per step), no flush",
                        "parallelism": f"row shards x{world}", "seed": SEED},
             "per_query": {
+                "filter_aggregate": {"ms": f_full, "fact_rows_per_s": n / (f_full / 1e3),
+                                     "gbs": n * 16 / f_full / 1e6, "frac_of_hbm": n * 16 / f_full / 1e6 / peak},
+                "filter_aggregate_6M": {"rows": f_small_rows, "ms": f_small,
+                                        "fact_rows_per_s": f_small_rows / (f_small / 1e3),
+                                        "gbs": f_small_rows * 16 / f_small / 1e6,
+                                        "frac_of_hbm": f_small_rows * 16 / f_small / 1e6 / peak,
+                                        "l2": "512 MB write before each launch"},
                 "A": {"probe_ms": pa, "fact_rows_per_s": n / (pa / 1e3), "gbs": n * QA_BYTES_PER_ROW / pa / 1e6,
                       "frac_of_hbm": n * QA_BYTES_PER_ROW / pa / 1e6 / peak},
                 "B": {"probe_ms": pb, "fact_rows_per_s": n / (pb / 1e3), "gbs": n * QB_BYTES_PER_ROW / pb / 1e6,
@@ -340,6 +462,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": f"star_kernel (Query {dom} probe)", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "algorithmic_bytes_per_launch": bytes_dom},
+            "batched": batched,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": launches,

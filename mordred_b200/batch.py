@@ -228,6 +228,70 @@ class BatchPlan:
         for a, _ in self.launches:
             L.check("mb_batch_run", L.lib().mb_batch_run(C.byref(a), st))
 
+    def set_launch(self, threads=0, items=0, stages=0, smem_group_bytes=-1) -> None:
+        """Change the launch configuration of every launch (0 / -1: the defaults)."""
+        for a, _ in self.launches:
+            a.threads, a.items_per_thread, a.stages = threads, items, stages
+            a.smem_group_bytes = smem_group_bytes
+
+    def capture(self, zero: torch.Tensor | None = None) -> torch.cuda.CUDAGraph:
+        """A CUDA graph of one run (preceded by zeroing `zero`, typically the buffer from
+        :func:`result_buffers`): the host-side planning and launch argument assembly happen
+        once, at capture; each replay is a handful of graph nodes."""
+        self.run()  # plan and load the kernels outside the capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            if zero is not None:
+                zero.zero_()
+            self.run()
+        return g
+
+    def autotune(self, configs=None, reps: int = 3) -> dict:
+        """Time launch configurations on this batch with CUDA events and keep the fastest.
+        Results are accumulated into while timing: zero them afterwards."""
+        configs = configs or BATCH_TUNE_CONFIGS
+        timings = []
+        for threads, items, stages, sg in configs:
+            self.set_launch(threads, items, stages, sg)
+            try:
+                self.run()
+            except L.MbError:
+                continue  # does not fit in shared memory
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                self.run()
+            e1.record()
+            torch.cuda.synchronize()
+            timings.append((e0.elapsed_time(e1) / reps, (threads, items, stages, sg)))
+        if not timings:
+            raise RuntimeError("no launch configuration fits this batch")
+        ms, best = min(timings)
+        self.set_launch(*best)
+        return {"best": dict(zip(("threads", "items", "stages", "smem_group_bytes"), best)), "ms": ms,
+                "timings": [(c, t) for t, c in timings]}
+
+
+# launch configurations the batch autotuner tries: consumer threads, rows per thread,
+# stages, shared memory for small group arrays
+BATCH_TUNE_CONFIGS = [(t, i, st, sg) for t, i in ((768, 1), (960, 1), (512, 2), (256, 4))
+                      for st in (2, 3) for sg in (65536, 131072)]
+
+
+def result_buffers(queries: list[Query], device="cuda") -> tuple[torch.Tensor, list[torch.Tensor]]:
+    """One zeroed buffer holding every query's result (so one memset clears a batch), and
+    per-query views of it shaped like :meth:`Query.result_buffer`."""
+    sizes = [8 if q.template == "agg" else 16 * q.groups for q in queries]
+    flat = torch.zeros(sum(sizes), dtype=torch.uint8, device=device)
+    views, off = [], 0
+    for q, nb in zip(queries, sizes):
+        v = flat[off: off + nb]
+        views.append(v.view(torch.int64) if q.template == "agg" else v.view(torch.int32))
+        off += nb
+    return flat, views
+
 
 def run_batch(t: dict, pats: Pats, queries: list[Query], results: list[torch.Tensor], n_rows: int,
               stream=None, threads=0, items=0, stages=0, smem_group_bytes=-1) -> None:

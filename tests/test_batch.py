@@ -140,3 +140,36 @@ def test_batch_wide_attributes_interval_and_table_paths():
         nonzero += exp != 0
     assert nonzero > 200
     assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
+def test_batch_graph_replay_and_autotune():
+    """A captured batch replays to the same results as a direct run, twice; the autotuner
+    picks a configuration that gives the same results too."""
+    import torch
+    from mordred_b200 import _lib as L
+    torch.cuda.set_device(0)
+    n = 3_000_017
+    s = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(s, 7, B.BATCH_FACT, B.BATCH_DIMS)
+    pats = B.build_pats(t, s)
+    qs = B.generate_queries(200, seed=8)
+    base = [q.result_buffer() for q in qs]
+    B.run_batch(t, pats, qs, base, n)
+    flat, views = B.result_buffers(qs)
+    plan = B.BatchPlan(t, pats, qs, views, n)
+    g = plan.capture(zero=flat)
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        for a, b in zip(views, base):
+            assert torch.equal(a.view(-1), b.view(-1))
+    info = plan.autotune(reps=1)
+    assert info["best"]["threads"] > 0 and len(info["timings"]) >= 2
+    flat.zero_()
+    plan.run()
+    torch.cuda.synchronize()
+    for a, b in zip(views, base):
+        assert torch.equal(a.view(-1), b.view(-1))
+    del g
+    assert L.device_status(0) == 0
