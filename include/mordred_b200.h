@@ -329,6 +329,29 @@ size_t mb_batch_workspace_bytes(const mb_batch_args* args);
  * persistent kernel scans the fact table once. */
 int mb_batch_run(const mb_batch_args* args, mb_stream_t stream);
 
+/* ---- CPU operators (host columns; the CPU half of CPU/GPU split execution) ------- */
+/* Host threads the CPU operators use at most (a persistent pool). */
+int mb_cpu_threads(void);
+
+/* Filtered perfect-hash build on the host: src/gpudb/CPUProcessing.cu:1034-1104
+ * build_CPU, and the Crystal layouts of mb_build_pht. layout MB_HT_KEY (dim_val unused),
+ * MB_HT_KEY_VAL {key, val} or MB_HT_VAL_OFF {val, row+1}. nthreads <= 0: all. Slots
+ * out of range set MB_STATUS_PROBE_RANGE in *status (optional). */
+int mb_cpu_build_pht(const int* filter_col, int filter_mode, int c1, int c2,
+                     const int* dim_key, const int* dim_val, int num_tuples,
+                     int* ht, int num_slots, int key_min, int layout, int nthreads,
+                     unsigned int* status);
+
+/* The fused star pipeline of mb_star_query over HOST columns and host hash tables
+ * (CPUProcessing.cu:439-568, 723-866, 1628-1710). gpu_cache must be NULL; segment_size
+ * > 0 maps virtual rows through segment_group as on the GPU, over plain host columns.
+ * rows (optional) lists the virtual rows to process (an offset list from
+ * mb_star_select); num_listed is its length. Results accumulate into args->res exactly
+ * as the GPU path's do, so CPU and GPU partial results of one query merge by addition
+ * (src/gpudb/CPUProcessing.cu:1786-1819 merge). Launch fields are ignored. */
+int mb_cpu_star_query(const mb_star_args* args, const int* rows, int64_t num_listed,
+                      int nthreads, unsigned int* status);
+
 /* ---- synthetic data (seeded; identical on host and device) ---------------------- */
 /* Fact column `col` (MB_LO_* in mordred_b200/csrc/ssbgen.h) rows [row0, row0+n) into a
  * device buffer. s_len/c_len/p_len give the foreign-key ranges. */

@@ -203,6 +203,9 @@ class MbBatchArgs(C.Structure):
 
 
 SIGNATURES.update({
+    "mb_cpu_threads": (I, []),
+    "mb_cpu_build_pht": (I, [P, I, I, I, P, P, I, P, I, I, I, I, PS(C.c_uint)]),
+    "mb_cpu_star_query": (I, [PS(MbStarArgs), P, I64, I, PS(C.c_uint)]),
     "mb_pat_build": (I, [P, I, I, I, P, I, P, I, P, I, P, P]),
     "mb_batch_workspace_bytes": (C.c_size_t, [PS(MbBatchArgs)]),
     "mb_batch_run": (I, [PS(MbBatchArgs), P]),

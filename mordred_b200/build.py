@@ -16,7 +16,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmordred_b200.so")
 
-SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "noalloc.cu", "batch.cu"]
+SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "noalloc.cu", "batch.cu", "cpu_engine.cpp"]
+# host code: portable x86-64 with AVX2 (the library is built on one machine and run on another)
+HOST_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-pthread"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -35,7 +37,7 @@ def _deps() -> list[str]:
     out = []
     for d in (CSRC, os.path.join(ROOT, "include")):
         for base, _, files in os.walk(d):
-            out += [os.path.join(base, f) for f in files if f.endswith((".cu", ".cuh", ".h"))]
+            out += [os.path.join(base, f) for f in files if f.endswith((".cu", ".cuh", ".h", ".cpp"))]
     return out
 
 
@@ -69,8 +71,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         common += ["-Xptxas", "-v"]
     jobs = []
     for src in _sources():
-        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        jobs.append(([*common, "-c", "-o", obj, src], obj))
+        stem, ext = os.path.splitext(os.path.basename(src))
+        obj = os.path.join(objdir, stem + ".o")
+        if ext == ".cpp":
+            jobs.append((["g++", *HOST_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", "-o", obj, src], obj))
+        else:
+            jobs.append(([*common, "-c", "-o", obj, src], obj))
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         logs = list(ex.map(lambda j: _run(j[0], verbose), jobs))
     if ptxas_verbose:
