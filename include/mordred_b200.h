@@ -352,6 +352,55 @@ int mb_cpu_build_pht(const int* filter_col, int filter_mode, int c1, int c2,
 int mb_cpu_star_query(const mb_star_args* args, const int* rows, int64_t num_listed,
                       int nthreads, unsigned int* status);
 
+/* ---- GPU segment cache (src/gpudb/CacheManager.{h,cu}) ---------------------------- */
+/* Fact columns are split into segments of segment_size rows (reference SEGMENT_SIZE,
+ * common.h:73). The cache owns one device pool of num_slots segment slots — the
+ * kernels' gpuCache — and maps (column, segment) to a slot. mb_segcache_col_idx gives
+ * a column's slot-per-segment array, the per-column index array of mb_star_query's
+ * segment addressing. device < 0 keeps the pool in host memory (bookkeeping without a
+ * GPU). Calls on one cache are serialised internally. */
+#define MB_CACHE_LRU 0     /* admission evicts the least recently used segment */
+#define MB_CACHE_LFU 1     /* ... the least frequently used */
+#define MB_CACHE_WEIGHT 2  /* ... the one with the smallest benefit weight */
+
+typedef struct mb_segcache mb_segcache;
+typedef struct mb_segcache_stats {
+  unsigned long long hits, misses;      /* mb_segcache_touch of resident / absent segments */
+  unsigned long long admissions, evictions, bytes_h2d;
+  unsigned long long resident;          /* slots in use */
+} mb_segcache_stats;
+
+/* NULL on bad arguments or when the pool cannot be allocated. num_segments <= 32767
+ * (segment ids are 16-bit in segment_group lists, as the reference's short). */
+mb_segcache* mb_segcache_create(int device, int64_t num_slots, int segment_size,
+                                int num_columns, int num_segments, int policy);
+void mb_segcache_destroy(mb_segcache* cache);
+int* mb_segcache_pool(mb_segcache* cache);
+/* Slot of (col, seg), -1 when not resident. */
+int mb_segcache_slot(mb_segcache* cache, int col, int seg);
+/* out[seg] = slot of (col, seg) or -1, for every segment (host array). */
+int mb_segcache_col_idx(mb_segcache* cache, int col, int* out);
+/* Start a query: segments it touches or admits from now on are pinned until the next
+ * mb_segcache_begin_query. */
+void mb_segcache_begin_query(mb_segcache* cache);
+/* Record a use of (col, seg) by the running query (recency, frequency, hit/miss). */
+int mb_segcache_touch(mb_segcache* cache, int col, int seg);
+int mb_segcache_set_weight(mb_segcache* cache, int col, int seg, double weight);
+/* Make (col, seg) resident, copying `rows` ints from host_src (pinned for asynchronous
+ * copies) on `stream`; evicts by the cache's policy when no slot is free (never a
+ * segment pinned by the running query: MB_ERR_SIZE when only those are left). */
+int mb_segcache_admit(mb_segcache* cache, int col, int seg, const int* host_src, int rows,
+                      mb_stream_t stream, int* slot_out);
+int mb_segcache_evict(mb_segcache* cache, int col, int seg);
+/* Epoch replacement (CacheManager.cu:534-588 SegmentReplacement): weights[col *
+ * num_segments + seg] are benefit weights; the positive ones, heaviest first, are made
+ * resident up to the slot count and every other resident segment is evicted.
+ * host_cols[col] is the host column (NULL: never admitted), segment_rows[seg] the rows
+ * of each segment. */
+int mb_segcache_replace(mb_segcache* cache, const double* weights, const int* const* host_cols,
+                        const int* segment_rows, mb_stream_t stream);
+int mb_segcache_get_stats(mb_segcache* cache, mb_segcache_stats* out);
+
 /* ---- synthetic data (seeded; identical on host and device) ---------------------- */
 /* Fact column `col` (MB_LO_* in mordred_b200/csrc/ssbgen.h) rows [row0, row0+n) into a
  * device buffer. s_len/c_len/p_len give the foreign-key ranges. */

@@ -14,6 +14,7 @@ from . import build as _build
 
 # ---- constants (mirror include/mordred_b200.h) -------------------------------------
 MB_OK = 0
+MB_ERR_ARG, MB_ERR_ALIGN, MB_ERR_LAUNCH, MB_ERR_CUDA, MB_ERR_NODEV, MB_ERR_SIZE = 1, 2, 3, 4, 5, 6
 MB_STATUS_PROBE_RANGE = 0x1
 MB_STATUS_GROUP_RANGE = 0x2
 MB_STATUS_TIMEOUT = 0x4
@@ -202,7 +203,26 @@ class MbBatchArgs(C.Structure):
                 ("stages", C.c_int), ("grid", C.c_int), ("smem_group_bytes", C.c_int)]
 
 
+MB_CACHE_LRU, MB_CACHE_LFU, MB_CACHE_WEIGHT = 0, 1, 2
+
+
+class MbSegcacheStats(C.Structure):
+    _fields_ = [(k, C.c_ulonglong) for k in ("hits", "misses", "admissions", "evictions", "bytes_h2d", "resident")]
+
+
 SIGNATURES.update({
+    "mb_segcache_create": (P, [I, I64, I, I, I, I]),
+    "mb_segcache_destroy": (None, [P]),
+    "mb_segcache_pool": (P, [P]),
+    "mb_segcache_slot": (I, [P, I, I]),
+    "mb_segcache_col_idx": (I, [P, I, P]),
+    "mb_segcache_begin_query": (None, [P]),
+    "mb_segcache_touch": (I, [P, I, I]),
+    "mb_segcache_set_weight": (I, [P, I, I, C.c_double]),
+    "mb_segcache_admit": (I, [P, I, I, P, I, P, PS(I)]),
+    "mb_segcache_evict": (I, [P, I, I]),
+    "mb_segcache_replace": (I, [P, P, P, P, P]),
+    "mb_segcache_get_stats": (I, [P, PS(MbSegcacheStats)]),
     "mb_cpu_threads": (I, []),
     "mb_cpu_build_pht": (I, [P, I, I, I, P, P, I, P, I, I, I, I, PS(C.c_uint)]),
     "mb_cpu_star_query": (I, [PS(MbStarArgs), P, I64, I, PS(C.c_uint)]),

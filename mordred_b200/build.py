@@ -16,10 +16,12 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmordred_b200.so")
 
-SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "noalloc.cu", "batch.cu", "cpu_engine.cpp"]
+SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "noalloc.cu", "batch.cu", "cpu_engine.cpp",
+           "segcache.cpp"]
 # host code: portable x86-64 with AVX2 (the library is built on one machine and run on another)
 HOST_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-pthread"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUDA_INCLUDE = "/usr/local/cuda/include"
 
 
 def nvcc() -> str:
@@ -74,7 +76,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         stem, ext = os.path.splitext(os.path.basename(src))
         obj = os.path.join(objdir, stem + ".o")
         if ext == ".cpp":
-            jobs.append((["g++", *HOST_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", "-o", obj, src], obj))
+            jobs.append((["g++", *HOST_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CUDA_INCLUDE, "-c", "-o",
+                          obj, src], obj))
         else:
             jobs.append(([*common, "-c", "-o", obj, src], obj))
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
