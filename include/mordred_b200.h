@@ -42,6 +42,7 @@ typedef void* mb_stream_t;
 #define MB_STATUS_PROBE_RANGE 0x1u  /* (key - key_min) % num_slots < 0: row treated as a miss */
 #define MB_STATUS_GROUP_RANGE 0x2u  /* group index outside [0, total_val): row skipped */
 #define MB_STATUS_TIMEOUT 0x4u      /* a bounded pipeline wait ran out; result incomplete */
+#define MB_STATUS_OVERFLOW 0x8u     /* an offset list was full: rows past its capacity were counted, not written */
 
 /* ---- enums ---------------------------------------------------------------------- */
 /* Filter modes: KernelArgs.h:44-86 (pred_eq, pred_between, pred_eq_or_eq),
@@ -328,6 +329,48 @@ size_t mb_batch_workspace_bytes(const mb_batch_args* args);
 /* Run a batch of queries: one small kernel fills the workspace's query masks, then one
  * persistent kernel scans the fact table once. */
 int mb_batch_run(const mb_batch_args* args, mb_stream_t stream);
+
+/* ---- selection with compaction: offset lists for CPU/GPU handoff ---------------- */
+/* KernelArgs.h:306-315 offsetGPU: a list of physical fact rows and, per dimension slot
+ * 1..4 (supplier, customer, part, date), the dimension offset each row joined with. */
+typedef struct mb_offsetGPU {
+  int* lo_off;
+  int* dim_off1; int* dim_off2; int* dim_off3; int* dim_off4;
+} mb_offsetGPU;
+
+/* Rows passing args' filters and probes (aggregation fields ignored) appended to an
+ * offset list: lo_off[k] = physical row (start_offset + row, or the segment-mapped row
+ * under segment addressing), dim_off[p][k] (optional per probe) = the probe's output:
+ * VAL_OFF tables give the dimension row (ht[2h+1] - 1), KEY_VAL tables the payload, KEY
+ * tables 0. *total (device int, zeroed by the caller) is the list cursor; entries past
+ * `capacity` are counted but not written and set MB_STATUS_OVERFLOW. in_rows (optional,
+ * device) restricts the pass to the listed physical rows (num_in of them). The order of
+ * the list is not deterministic; its set of rows is. Restates filter_probe_GPU2/3,
+ * probe_GPU2/3 and filter_GPU2/3 (src/gpudb/GPUProcessing.h:496-925, 1174-1383). */
+int mb_star_select(const mb_star_args* args, const int* in_rows, int64_t num_in, int* lo_off,
+                   int* const* dim_off, int64_t capacity, int* total, mb_stream_t stream);
+
+/* The engine forms over the segment cache (SEGMENT_SIZE 1,048,576): column fields are
+ * per-segment slot-index arrays into gpuCache; probes use engine (VAL_OFF) tables for
+ * each dimension slot whose key_idx and ht are both set; out_off arrays hold
+ * num_tuples entries. The GPU3 forms take the physical rows of in_off->lo_off and pass
+ * in_off's dimension offsets through to slots they do not probe. */
+int mb_filter_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_offsetGPU* out_off,
+                   int num_tuples, int* total, int start_offset, const short* segment_group,
+                   mb_stream_t stream);
+int mb_filter_probe_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_probeArgsGPU* pargs,
+                         const mb_offsetGPU* out_off, int num_tuples, int* total, int start_offset,
+                         const short* segment_group, mb_stream_t stream);
+int mb_probe_GPU2(const int* gpuCache, const mb_probeArgsGPU* pargs, const mb_offsetGPU* out_off,
+                  int num_tuples, int* total, int start_offset, const short* segment_group,
+                  mb_stream_t stream);
+int mb_filter_GPU3(const int* gpuCache, const mb_offsetGPU* in_off, const mb_filterArgsGPU* fargs,
+                   const mb_offsetGPU* out_off, int num_tuples, int* total, mb_stream_t stream);
+int mb_filter_probe_GPU3(const int* gpuCache, const mb_offsetGPU* in_off, const mb_filterArgsGPU* fargs,
+                         const mb_probeArgsGPU* pargs, const mb_offsetGPU* out_off, int num_tuples,
+                         int* total, mb_stream_t stream);
+int mb_probe_GPU3(const int* gpuCache, const mb_offsetGPU* in_off, const mb_probeArgsGPU* pargs,
+                  const mb_offsetGPU* out_off, int num_tuples, int* total, mb_stream_t stream);
 
 /* ---- CPU operators (host columns; the CPU half of CPU/GPU split execution) ------- */
 /* Host threads the CPU operators use at most (a persistent pool). */

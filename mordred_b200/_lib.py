@@ -18,6 +18,7 @@ MB_ERR_ARG, MB_ERR_ALIGN, MB_ERR_LAUNCH, MB_ERR_CUDA, MB_ERR_NODEV, MB_ERR_SIZE 
 MB_STATUS_PROBE_RANGE = 0x1
 MB_STATUS_GROUP_RANGE = 0x2
 MB_STATUS_TIMEOUT = 0x4
+MB_STATUS_OVERFLOW = 0x8
 
 MB_FILTER_EQ, MB_FILTER_BETWEEN, MB_FILTER_EQ_OR_EQ = 0, 1, 2
 MB_HT_KEY, MB_HT_KEY_VAL, MB_HT_VAL_OFF = 0, 1, 2
@@ -210,7 +211,19 @@ class MbSegcacheStats(C.Structure):
     _fields_ = [(k, C.c_ulonglong) for k in ("hits", "misses", "admissions", "evictions", "bytes_h2d", "resident")]
 
 
+class MbOffsetGPU(C.Structure):
+    _fields_ = [("lo_off", C.c_void_p)] + [(f"dim_off{i}", C.c_void_p) for i in range(1, 5)]
+
+
 SIGNATURES.update({
+    "mb_star_select": (I, [PS(MbStarArgs), P, I64, P, P, I64, P, P]),
+    "mb_filter_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbOffsetGPU), I, P, I, P, P]),
+    "mb_filter_probe_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P, I, P, P]),
+    "mb_probe_GPU2": (I, [P, PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P, I, P, P]),
+    "mb_filter_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbFilterArgsGPU), PS(MbOffsetGPU), I, P, P]),
+    "mb_filter_probe_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbFilterArgsGPU), PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P,
+                                 P]),
+    "mb_probe_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P, P]),
     "mb_segcache_create": (P, [I, I64, I, I, I, I]),
     "mb_segcache_destroy": (None, [P]),
     "mb_segcache_pool": (P, [P]),
