@@ -372,6 +372,28 @@ int mb_filter_probe_GPU3(const int* gpuCache, const mb_offsetGPU* in_off, const 
 int mb_probe_GPU3(const int* gpuCache, const mb_offsetGPU* in_off, const mb_probeArgsGPU* pargs,
                   const mb_offsetGPU* out_off, int num_tuples, int* total, mb_stream_t stream);
 
+/* ---- learned planner: the cost MLP (no counterpart kernel in the reference, which
+ * plans with the analytic model of src/gpudb/CostModel.cu:283-440) ------------------- */
+/* 24 features -> 64 -> 64 -> 2 outputs (predicted log CPU ms, log GPU ms of a segment),
+ * ReLU, fp32. params: W1[24][64], b1[64], W2[64][64], b2[64], W3[64][2], b3[2] (W[i][j]:
+ * input i -> unit j), 5,890 floats. All pointers are device pointers. */
+#define MB_MLP_IN 24
+#define MB_MLP_HIDDEN 64
+#define MB_MLP_OUT 2
+#define MB_MLP_PARAMS 5890
+/* y[batch][2] = MLP(x[batch][24]). */
+int mb_mlp_forward(const float* params, const float* x, int batch, float* y, mb_stream_t stream);
+/* grads[5890] += d/dparams of 1/(2*batch) * sum (MLP(x) - target)^2 (grads zeroed by the
+ * caller); loss_sum (optional) += 1/2 * sum (MLP(x) - target)^2. Gradients are summed
+ * with fp32 atomics, so their last bits vary between runs. */
+int mb_mlp_backward(const float* params, const float* x, const float* target, int batch,
+                    float* grads, float* loss_sum, mb_stream_t stream);
+/* One Adam step on n parameters (an L2 term weight_decay * param is added to each
+ * gradient first); step counts from 1. */
+int mb_mlp_adam(float* params, const float* grads, float* m, float* v, int n, float lr,
+                float beta1, float beta2, float eps, int step, float weight_decay,
+                mb_stream_t stream);
+
 /* ---- CPU operators (host columns; the CPU half of CPU/GPU split execution) ------- */
 /* Host threads the CPU operators use at most (a persistent pool). */
 int mb_cpu_threads(void);

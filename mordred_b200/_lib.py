@@ -215,7 +215,13 @@ class MbOffsetGPU(C.Structure):
     _fields_ = [("lo_off", C.c_void_p)] + [(f"dim_off{i}", C.c_void_p) for i in range(1, 5)]
 
 
+MB_MLP_IN, MB_MLP_HIDDEN, MB_MLP_OUT, MB_MLP_PARAMS = 24, 64, 2, 5890
+F32 = C.c_float
+
 SIGNATURES.update({
+    "mb_mlp_forward": (I, [P, P, I, P, P]),
+    "mb_mlp_backward": (I, [P, P, P, I, P, P, P]),
+    "mb_mlp_adam": (I, [P, P, P, P, I, F32, F32, F32, F32, I, F32, P]),
     "mb_star_select": (I, [PS(MbStarArgs), P, I64, P, P, I64, P, P]),
     "mb_filter_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbOffsetGPU), I, P, I, P, P]),
     "mb_filter_probe_GPU2": (I, [P, PS(MbFilterArgsGPU), PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P, I, P, P]),
