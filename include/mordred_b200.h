@@ -394,6 +394,33 @@ int mb_mlp_adam(float* params, const float* grads, float* m, float* v, int n, fl
                 float beta1, float beta2, float eps, int step, float weight_decay,
                 mb_stream_t stream);
 
+/* ---- analytic cost model and segment placement (src/gpudb/CostModel.{h,cu}) ------- */
+/* A fact pipeline for costing: filters, then probes, then (optionally) a group-by or
+ * aggregate over num_aggr columns, with the fraction of rows each filter / probe keeps. */
+typedef struct mb_cost_pipeline {
+  int num_filters;
+  double filter_sel[MB_MAX_FILTERS];
+  int num_probes;
+  double probe_sel[MB_MAX_PROBES];
+  int group_by;   /* 1: a group-by / aggregate ends the pipeline */
+  int num_aggr;   /* its aggregate columns (n_aggr_key) */
+} mb_cost_pipeline;
+
+/* CostModel.cu:283-363 calculate_cost for one placement: on_gpu[i] for the filters,
+ * then the probes, then the group-by (1 = GPU). Returns ms (BW_CPU 42e6 and BW_PCI
+ * 12e6 bytes per ms, CostModel.h:4-6) for `rows` rows, or -1 on bad arguments. */
+double mb_cost_calculate(const mb_cost_pipeline* pipeline, const int* on_gpu, double rows);
+/* The whole pipeline on the CPU. */
+double mb_cost_cpu_ms(const mb_cost_pipeline* pipeline, double rows);
+/* CostModel.cu:386-390 transfer_cost: `columns` int columns of `rows` rows over PCIe. */
+double mb_cost_transfer_ms(double rows, int columns);
+/* Split n segments between CPU and GPU (on_gpu[i] = 1: GPU) to minimise
+ * max(sum of GPU ms, sum of CPU ms) over a GPU/CPU time-ratio order; *makespan_ms
+ * (optional) receives that maximum. No counterpart in the reference, which places by
+ * segment residency (QueryOptimizer.cu:1674-1891). */
+int mb_place_segments(int n, const double* cpu_ms, const double* gpu_ms, unsigned char* on_gpu,
+                      double* makespan_ms);
+
 /* ---- CPU operators (host columns; the CPU half of CPU/GPU split execution) ------- */
 /* Host threads the CPU operators use at most (a persistent pool). */
 int mb_cpu_threads(void);

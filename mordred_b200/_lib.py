@@ -218,7 +218,16 @@ class MbOffsetGPU(C.Structure):
 MB_MLP_IN, MB_MLP_HIDDEN, MB_MLP_OUT, MB_MLP_PARAMS = 24, 64, 2, 5890
 F32 = C.c_float
 
+class MbCostPipeline(C.Structure):
+    _fields_ = [("num_filters", C.c_int), ("filter_sel", C.c_double * MB_MAX_FILTERS), ("num_probes", C.c_int),
+                ("probe_sel", C.c_double * MB_MAX_PROBES), ("group_by", C.c_int), ("num_aggr", C.c_int)]
+
+
 SIGNATURES.update({
+    "mb_cost_calculate": (C.c_double, [PS(MbCostPipeline), PS(C.c_int), C.c_double]),
+    "mb_cost_cpu_ms": (C.c_double, [PS(MbCostPipeline), C.c_double]),
+    "mb_cost_transfer_ms": (C.c_double, [C.c_double, C.c_int]),
+    "mb_place_segments": (I, [I, P, P, P, P]),
     "mb_mlp_forward": (I, [P, P, I, P, P]),
     "mb_mlp_backward": (I, [P, P, P, I, P, P, P]),
     "mb_mlp_adam": (I, [P, P, P, P, I, F32, F32, F32, F32, I, F32, P]),

@@ -1,0 +1,62 @@
+"""The analytic cost model against its restatement and a hand-computed case, and the
+CPU/GPU segment placement against an exhaustive search over its candidate splits."""
+import ctypes as C
+import itertools
+
+import numpy as np
+import pytest
+
+from mordred_b200 import _lib as L
+from oracle import cost_oracle as CO
+
+
+def _pipe(fs, ps, group_by=1, n_aggr=2):
+    p = L.MbCostPipeline()
+    p.num_filters, p.num_probes, p.group_by, p.num_aggr = len(fs), len(ps), group_by, n_aggr
+    for i, s in enumerate(fs):
+        p.filter_sel[i] = s
+    for i, s in enumerate(ps):
+        p.probe_sel[i] = s
+    return p
+
+
+def test_hand_computed_all_cpu():
+    # 1e6 rows: filter 0.3 keeps 3e5; probe 0.2 keeps 6e4; group over 2 aggregate columns
+    p = _pipe([0.3], [0.2])
+    exp = 1e6 * 4 / 42e6 + (3e5 * 4 / 42e6 + 3e5 * 64 / 42e6) + (6e4 * 64 * 2 / 42e6 + 6e4 * 64 / 42e6)
+    assert abs(L.lib().mb_cost_cpu_ms(C.byref(p), 1e6) - exp) < 1e-12
+    assert abs(L.lib().mb_cost_transfer_ms(1e6, 3) - 1e6 * 12 / 12e6) < 1e-12
+
+
+def test_every_placement_matches_restatement():
+    rng = np.random.default_rng(0)
+    for _ in range(40):
+        fs = list(rng.uniform(0.01, 1, rng.integers(0, 4)))
+        ps = list(rng.uniform(0.01, 1, rng.integers(0, 5)))
+        g = int(rng.integers(0, 2))
+        p = _pipe(fs, ps, g, int(rng.integers(1, 3)))
+        nops = len(fs) + len(ps) + 1
+        for dev in itertools.product([0, 1], repeat=nops):
+            arr = (C.c_int * nops)(*dev)
+            got = L.lib().mb_cost_calculate(C.byref(p), arr, 2.5e6)
+            exp = CO.calculate_cost(fs, ps, g, p.num_aggr, list(dev), 2.5e6)
+            assert abs(got - exp) <= 1e-9 * max(1.0, abs(exp)), (fs, ps, g, dev)
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 7, 40])
+def test_placement_is_best_split_of_ratio_order(n):
+    rng = np.random.default_rng(n)
+    cpu = rng.uniform(0.1, 5, n)
+    gpu = rng.uniform(0.0, 3, n)
+    on = np.zeros(n, np.uint8)
+    span = C.c_double(0)
+    L.call("mb_place_segments", n, cpu.ctypes.data, gpu.ctypes.data, on.ctypes.data, C.byref(span))
+    got = max(gpu[on == 1].sum(), cpu[on == 0].sum()) if n else 0.0
+    assert abs(got - span.value) < 1e-9
+    order = np.argsort(gpu / cpu, kind="stable")
+    best = min(max(gpu[order[:k]].sum(), cpu[order[k:]].sum()) for k in range(n + 1)) if n else 0.0
+    assert abs(span.value - best) < 1e-9
+    if n <= 10 and n > 0:  # and near the true optimum over all 2^n assignments
+        opt = min(max(gpu[np.array(m, bool)].sum(), cpu[~np.array(m, bool)].sum())
+                  for m in itertools.product([0, 1], repeat=n))
+        assert span.value <= opt + max(gpu.max(), cpu.max())
