@@ -1,0 +1,433 @@
+"""Segmented execution of star queries over a host-resident fact table: segment skipping,
+a GPU segment cache, CPU/GPU placement by a planner, concurrent CPU and GPU halves, and
+the merge of their results.
+
+Restates the reference's executor path for one query (src/gpudb/QueryProcessing.cu:
+runQuery :1347-1471, executeTableDim :109-152, executeTableFact_v1 :201-437) on the
+library's operators:
+
+* :class:`SegmentedTable` — the fact table in pinned host memory, sorted by orderdate
+  (as the reference's LINEORDERSORT files, src/gpudb/common.h:110-135) and split into
+  segments of 1,048,576 rows (common.h:73), with per-segment min/max of every column
+  (minmax.cpp:28-45); dimension tables on the GPU and the host.
+* :class:`Executor` — per query: skip segments whose orderdate range misses the query's
+  (QueryOptimizer.cu:1641-1662 checkPredicate); ask the planner for each remaining
+  segment's CPU and GPU milliseconds and split them (mb_place_segments); run the GPU
+  share from the segment cache (missing column segments admitted on the query's stream,
+  in waves when the cache cannot hold them all at once) with one fused launch per wave,
+  and concurrently the CPU share with the CPU engine over the pinned host columns; add
+  the two partial results (CPUProcessing.cu:1786-1819 merge).
+* :meth:`Executor.profile_segments` — per-segment timings on each device, the log the
+  learned planner trains on.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import batch as B
+from . import cpu, ssb
+from .planner import SegmentContext, features, place, analytic_ms
+from .segcache import SegmentCache
+
+SEG = 1 << 20
+FACT = list(B.BATCH_FACT)                      # column id = index (the cache's column numbering)
+COL_ID = {name: i for i, name in enumerate(FACT)}
+NEEDED = {"agg": ["lo_orderdate", "lo_discount", "lo_quantity", "lo_extendedprice"],
+          "qa": ["lo_orderdate", "lo_suppkey", "lo_partkey", "lo_revenue"],
+          "qb": ["lo_orderdate", "lo_suppkey", "lo_custkey", "lo_partkey", "lo_revenue", "lo_supplycost"]}
+DIMS = ["d_datekey", "d_year", "s_suppkey", "s_region", "c_custkey", "c_region", "c_nation", "p_partkey", "p_mfgr",
+        "p_category", "p_brand1"]
+CAL = np.array(B.CALENDAR, dtype=np.int64)
+DAY_OF = {d: i for i, d in enumerate(B.CALENDAR)}
+
+
+def _day(date: int) -> int:
+    """Index of a yyyymmdd value in the calendar (dates between calendar days round up)."""
+    return int(np.searchsorted(CAL, date))
+
+
+class SegmentedTable:
+    """n fact rows (the batch columns) in pinned host memory, orderdate ascending: row r
+    has calendar day floor(r * 2557 / n), every other column from the seeded generator."""
+
+    def __init__(self, n_rows: int, seed: int, sizes: ssb.Sizes | None = None, device="cuda",
+                 columns: list[str] | None = None):
+        self.n = n_rows
+        self.nseg = (n_rows + SEG - 1) // SEG
+        if self.nseg > 32767:
+            raise ValueError("at most 32,767 segments")
+        self.seg_rows = np.full(self.nseg, SEG, np.int32)
+        self.seg_rows[-1] = n_rows - (self.nseg - 1) * SEG
+        self.sizes = sizes or ssb.Sizes(lo_len=n_rows)
+        self.seed = seed
+        self.columns = columns or FACT
+        self.host_t = {}
+        self.host = {}
+        self.min = {}
+        self.max = {}
+        st = ssb._stream()
+        chunk = 64 * SEG
+        buf = torch.empty(chunk, dtype=torch.int32, device=device)
+        cal = torch.tensor(CAL, dtype=torch.int32, device=device)
+        for name in self.columns:
+            h = torch.empty(n_rows, dtype=torch.int32, pin_memory=True)
+            mins = np.empty(self.nseg, np.int32)
+            maxs = np.empty(self.nseg, np.int32)
+            for r0 in range(0, n_rows, chunk):
+                cnt = min(chunk, n_rows - r0)
+                if name == "lo_orderdate":
+                    r = torch.arange(r0, r0 + cnt, dtype=torch.int64, device=device)
+                    buf[:cnt] = cal[(r * len(CAL)) // n_rows]
+                else:
+                    L.call("mb_gen_fact_column", ssb.FACT_COLUMNS[name], seed, r0, cnt, self.sizes.s_len,
+                           self.sizes.c_len, self.sizes.p_len, buf.data_ptr(), st)
+                full = cnt // SEG
+                s0 = r0 // SEG
+                if full:
+                    v = buf[: full * SEG].view(full, SEG)
+                    mins[s0: s0 + full] = v.amin(1).cpu().numpy()
+                    maxs[s0: s0 + full] = v.amax(1).cpu().numpy()
+                if cnt % SEG:
+                    v = buf[full * SEG: cnt]
+                    mins[s0 + full], maxs[s0 + full] = int(v.min()), int(v.max())
+                h[r0: r0 + cnt].copy_(buf[:cnt])
+            self.host_t[name] = h
+            self.host[name] = h.numpy()
+            self.min[name], self.max[name] = mins, maxs
+        del buf
+        self.dims = ssb.gen_device(self.sizes, seed, [], DIMS)
+        self.hdims = {k: v.cpu().numpy() for k, v in self.dims.items()}
+        self.seg_day_lo = np.array([_day(int(x)) for x in self.min["lo_orderdate"]])
+        self.seg_day_hi = np.array([_day(int(x)) for x in self.max["lo_orderdate"]])
+
+    def ptr(self, name: str, seg: int) -> int:
+        return self.host[name].ctypes.data + seg * SEG * 4
+
+
+def _small_sel(q: B.Query) -> dict:
+    w = lambda r, n: (r[1] - r[0] + 1) / n
+    out = {"discount": 1.0, "quantity": 1.0, "s": 1.0, "c": 1.0, "p": 1.0}
+    if q.template == "agg":
+        out["discount"], out["quantity"] = w(q.discount, 11), w(q.quantity, 50)
+    elif q.template == "qa":
+        out["s"], out["p"] = w(q.s_region, 5), w(q.category, 25)
+    else:
+        out["s"], out["c"], out["p"] = w(q.s_region, 5), w(q.c_region, 5), w(q.mfgr, 5)
+    return out
+
+
+@dataclass
+class QueryRun:
+    """Outcome of one query: its result array (host), timings and placement."""
+    result: np.ndarray
+    ms: float
+    candidates: int
+    skipped: int
+    gpu_segments: int
+    cpu_segments: int
+    waves: int
+    predicted_makespan_ms: float
+    gpu_ms: float = 0.0
+    cpu_ms: float = 0.0
+    admitted: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+class Executor:
+    def __init__(self, table: SegmentedTable, cache_slots: int = 2048, policy: str = "lru", device: int = 0,
+                 max_waves: int = 16):
+        self.t = table
+        self.cache = SegmentCache(cache_slots, SEG, len(FACT), table.nseg, policy, device)
+        s = table.sizes
+        z = lambda n: torch.zeros(n, dtype=torch.int32, device="cuda")
+        self.ht = {"s": z(s.s_len), "c": z(2 * s.c_len), "p_key": z(s.p_len), "p_kv": z(2 * s.p_len),
+                   "d": z(2 * ssb.DATE_SLOTS)}
+        self.hht = {k: np.zeros(v.numel(), np.int32) for k, v in self.ht.items()}
+        self.max_waves = max_waves
+        self.col_idx_h = torch.empty(max_waves, len(FACT), table.nseg, dtype=torch.int32, pin_memory=True)
+        self.col_idx_d = torch.empty(max_waves, len(FACT), table.nseg, dtype=torch.int32, device="cuda")
+        self.seg_h = torch.empty(max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
+        self.seg_d = torch.empty(max_waves, table.nseg, dtype=torch.int16, device="cuda")
+        self.res_d = torch.zeros(4 * ssb.QA_GROUPS, dtype=torch.int32, device="cuda")
+        self.res_h = torch.empty(4 * ssb.QA_GROUPS, dtype=torch.int32, pin_memory=True)
+        self.cpu_threads = cpu.threads()
+        # the day-0 date key of the table's date dimension (for the date probe's slots)
+        self.date_slots = ssb.DATE_SLOTS
+
+    # ---- planning inputs ----------------------------------------------------------------
+    def candidates(self, q: B.Query) -> np.ndarray:
+        """Segments whose orderdate [min, max] meets the query's range (and, for the
+        filter-aggregate, whose discount and quantity ranges meet the query's)."""
+        t = self.t
+        ok = (t.max["lo_orderdate"] >= q.date[0]) & (t.min["lo_orderdate"] <= q.date[1])
+        if q.template == "agg":
+            for name, r in (("lo_discount", q.discount), ("lo_quantity", q.quantity)):
+                if name in t.min:
+                    ok &= (t.max[name] >= r[0]) & (t.min[name] <= r[1])
+        return np.nonzero(ok)[0]
+
+    def context(self, q: B.Query, seg: int, small: dict) -> SegmentContext:
+        t = self.t
+        lo, hi = t.seg_day_lo[seg], t.seg_day_hi[seg]
+        qlo, qhi = _day(q.date[0]), _day(q.date[1] + 1) - 1
+        inter = max(0, min(hi, qhi) - max(lo, qlo) + 1)
+        date_sel = inter / max(1, hi - lo + 1)
+        need = NEEDED[q.template]
+        res = sum(self.cache.slot(COL_ID[c], int(seg)) >= 0 for c in need)
+        s = t.sizes
+        ht_bytes = {"agg": 0, "qa": 4 * (s.s_len + 2 * s.p_len + 2 * ssb.DATE_SLOTS),
+                    "qb": 4 * (s.s_len + 2 * s.c_len + s.p_len + 2 * ssb.DATE_SLOTS)}[q.template]
+        free = 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
+        return SegmentContext(q.template, int(t.seg_rows[seg]), float(date_sel), small, len(need), int(res),
+                              ht_bytes, q.groups, self.cpu_threads, free)
+
+    # ---- builds ------------------------------------------------------------------------
+    def build_gpu(self, q: B.Query) -> None:
+        if q.template == "agg":
+            return
+        d, s, st = self.t.dims, self.t.sizes, ssb._stream()
+        BT = L.MB_FILTER_BETWEEN
+        self.ht["s"].zero_()
+        self.ht["d"].zero_()
+        L.call("mb_build_pht", ssb._p(d["s_region"]), BT, q.s_region[0], q.s_region[1], ssb._p(d["s_suppkey"]), None,
+               s.s_len, ssb._p(self.ht["s"]), s.s_len, 0, None, st)
+        L.call("mb_build_pht", None, 0, 0, 0, ssb._p(d["d_datekey"]), ssb._p(d["d_year"]), s.d_len,
+               ssb._p(self.ht["d"]), ssb.DATE_SLOTS, ssb.DATE_MIN, None, st)
+        if q.template == "qa":
+            self.ht["p_kv"].zero_()
+            L.call("mb_build_pht", ssb._p(d["p_category"]), BT, q.category[0], q.category[1], ssb._p(d["p_partkey"]),
+                   ssb._p(d["p_brand1"]), s.p_len, ssb._p(self.ht["p_kv"]), s.p_len, 0, None, st)
+        else:
+            self.ht["c"].zero_()
+            self.ht["p_key"].zero_()
+            L.call("mb_build_pht", ssb._p(d["c_region"]), BT, q.c_region[0], q.c_region[1], ssb._p(d["c_custkey"]),
+                   ssb._p(d["c_nation"]), s.c_len, ssb._p(self.ht["c"]), s.c_len, 0, None, st)
+            L.call("mb_build_pht", ssb._p(d["p_mfgr"]), BT, q.mfgr[0], q.mfgr[1], ssb._p(d["p_partkey"]), None,
+                   s.p_len, ssb._p(self.ht["p_key"]), s.p_len, 0, None, st)
+
+    def build_cpu(self, q: B.Query) -> None:
+        if q.template == "agg":
+            return
+        d, s, h = self.t.hdims, self.t.sizes, self.hht
+        BT = L.MB_FILTER_BETWEEN
+        h["s"][:] = 0
+        h["d"][:] = 0
+        cpu.build_pht(d["s_region"], BT, q.s_region[0], q.s_region[1], d["s_suppkey"], None, h["s"], s.s_len, 0,
+                      L.MB_HT_KEY)
+        cpu.build_pht(None, 0, 0, 0, d["d_datekey"], d["d_year"], h["d"], ssb.DATE_SLOTS, ssb.DATE_MIN,
+                      L.MB_HT_KEY_VAL)
+        if q.template == "qa":
+            h["p_kv"][:] = 0
+            cpu.build_pht(d["p_category"], BT, q.category[0], q.category[1], d["p_partkey"], d["p_brand1"], h["p_kv"],
+                          s.p_len, 0, L.MB_HT_KEY_VAL)
+        else:
+            h["c"][:] = 0
+            h["p_key"][:] = 0
+            cpu.build_pht(d["c_region"], BT, q.c_region[0], q.c_region[1], d["c_custkey"], d["c_nation"], h["c"],
+                          s.c_len, 0, L.MB_HT_KEY_VAL)
+            cpu.build_pht(d["p_mfgr"], BT, q.mfgr[0], q.mfgr[1], d["p_partkey"], None, h["p_key"], s.p_len, 0,
+                          L.MB_HT_KEY)
+
+    # ---- the fused pipeline's arguments --------------------------------------------------
+    def args(self, q: B.Query, col, ht: dict, n_rows: int, res, **extra) -> L.MbStarArgs:
+        """mb_star_args of query q; col(name) gives a column (pointer or array), ht the tables."""
+        s = self.t.sizes
+        BT = L.MB_FILTER_BETWEEN
+        date = dict(col=col("lo_orderdate"), mode=BT, c1=q.date[0], c2=q.date[1])
+        d_probe = dict(fkey=col("lo_orderdate"), ht=ht["d"], num_slots=ssb.DATE_SLOTS, key_min=ssb.DATE_MIN,
+                       layout=L.MB_HT_KEY_VAL, min_val=1992, unique_val=1, res_slot=0)
+        s_probe = dict(fkey=col("lo_suppkey"), ht=ht["s"], num_slots=s.s_len, layout=L.MB_HT_KEY)
+        if q.template == "agg":
+            return ssb.star_args(num_rows=n_rows, filters=[
+                date, dict(col=col("lo_discount"), mode=BT, c1=q.discount[0], c2=q.discount[1]),
+                dict(col=col("lo_quantity"), mode=BT, c1=q.quantity[0], c2=q.quantity[1])],
+                aggr=[col("lo_extendedprice"), col("lo_discount")], agg_op=L.MB_AGG_MUL,
+                res_layout=L.MB_RES_SCALAR, res=res, **extra)
+        if q.template == "qa":
+            probes = [s_probe, dict(fkey=col("lo_partkey"), ht=ht["p_kv"], num_slots=s.p_len, layout=L.MB_HT_KEY_VAL,
+                                    unique_val=7, res_slot=1), d_probe]
+            return ssb.star_args(num_rows=n_rows, filters=[date], probes=probes, aggr=[col("lo_revenue")],
+                                 agg_op=L.MB_AGG_SUM, total_val=ssb.QA_GROUPS, res_layout=L.MB_RES_CRYSTAL4, res=res,
+                                 **extra)
+        probes = [s_probe, dict(fkey=col("lo_custkey"), ht=ht["c"], num_slots=s.c_len, layout=L.MB_HT_KEY_VAL,
+                                unique_val=7, res_slot=1),
+                  dict(fkey=col("lo_partkey"), ht=ht["p_key"], num_slots=s.p_len, layout=L.MB_HT_KEY), d_probe]
+        return ssb.star_args(num_rows=n_rows, filters=[date], probes=probes,
+                             aggr=[col("lo_revenue"), col("lo_supplycost")], agg_op=L.MB_AGG_SUB,
+                             total_val=ssb.QB_GROUPS, res_layout=L.MB_RES_CRYSTAL4, res=res, **extra)
+
+    @staticmethod
+    def _order(segs: np.ndarray, t: SegmentedTable) -> np.ndarray:
+        """A segment list with the table's partial last segment (if listed) at the end."""
+        segs = np.asarray(segs, np.int64)
+        last = t.nseg - 1
+        if t.seg_rows[last] != SEG and (segs == last).any():
+            segs = np.concatenate([segs[segs != last], [last]])
+        return segs
+
+    def _rows(self, segs: np.ndarray) -> int:
+        return int(self.t.seg_rows[segs].sum())
+
+    def _launch_wave(self, q: B.Query, segs: list[int], w: int) -> None:
+        segs = self._order(np.array(segs), self.t)
+        for c in range(len(FACT)):
+            L.call("mb_segcache_col_idx", self.cache.h, c, self.col_idx_h[w, c].data_ptr())
+        self.seg_h[w, : len(segs)] = torch.from_numpy(segs.astype(np.int16))
+        self.col_idx_d[w].copy_(self.col_idx_h[w], non_blocking=True)
+        self.seg_d[w, : len(segs)].copy_(self.seg_h[w, : len(segs)], non_blocking=True)
+        col = lambda name: self.col_idx_d[w, COL_ID[name]]
+        a = self.args(q, col, self.ht, self._rows(segs), self.res_d, gpu_cache=self.cache.pool,
+                      segment_group=self.seg_d[w], segment_size=SEG)
+        ssb.star_query(a)
+
+    def _admit(self, q: B.Query, seg: int, st: int) -> int:
+        """Make the query's columns of `seg` resident (pinned for the running query);
+        returns the column segments copied. Raises MbError(MB_ERR_SIZE) when the cache
+        is full of pinned segments."""
+        n = 0
+        for c in (COL_ID[x] for x in NEEDED[q.template]):
+            self.cache.touch(c, seg)
+            if self.cache.slot(c, seg) < 0:
+                self.cache.admit(c, seg, self.t.ptr(FACT[c], seg), int(self.t.seg_rows[seg]), st)
+                n += 1
+        return n
+
+    def _gpu_half(self, q: B.Query, gsegs: list[int]) -> tuple[int, int, list[int]]:
+        """Enqueue the GPU share on the current stream: builds, admissions, one fused
+        launch per wave. Returns (waves, column segments admitted, segments left over)."""
+        st = ssb._stream()
+        self.build_gpu(q)
+        waves: list[list[int]] = [[]]
+        admitted = 0
+        left: list[int] = []
+        for sgi in gsegs:
+            try:
+                admitted += self._admit(q, sgi, st)
+                waves[-1].append(sgi)
+                continue
+            except L.MbError as e:
+                if e.code != L.MB_ERR_SIZE or not waves[-1] or len(waves) == self.max_waves:
+                    left.append(sgi)
+                    continue
+            # the cache is full of this wave's segments: launch it, then unpin it so the next
+            # wave may recycle its slots (copies into them are ordered after its kernel on
+            # this stream)
+            self._launch_wave(q, waves[-1], len(waves) - 1)
+            waves.append([])
+            self.cache.begin_query()
+            try:
+                admitted += self._admit(q, sgi, st)
+                waves[-1].append(sgi)
+            except L.MbError:
+                left.append(sgi)
+        if waves[-1]:
+            self._launch_wave(q, waves[-1], len(waves) - 1)
+        else:
+            waves.pop()
+        return len(waves), admitted, left
+
+    def _cpu_half(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
+        self.build_cpu(q)
+        segs = self._order(np.array(csegs), self.t)
+        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res,
+                      segment_group=segs.astype(np.int16), segment_size=SEG)
+        cpu.star_query(a)
+
+    # ---- one query -----------------------------------------------------------------------
+    def run(self, q: B.Query, planner, on_gpu: np.ndarray | None = None) -> QueryRun:
+        """Run q with `planner` placing its segments (or the given placement); returns the
+        merged result and timings. The GPU share is enqueued first (it only issues
+        asynchronous work), then the CPU share runs on this thread's pool while the GPU
+        works; the CPU also takes GPU segments the cache could not hold."""
+        t0 = time.perf_counter()
+        cand = self.candidates(q)
+        small = _small_sel(q)
+        self.cache.begin_query()
+        span = float("nan")
+        if on_gpu is None:
+            ctxs = [self.context(q, int(s), small) for s in cand]
+            pc, pg = planner.predict(ctxs)
+            on_gpu, span = place(pc, pg)
+        gsegs = [int(s) for s in cand[on_gpu]]
+        csegs = [int(s) for s in cand[~on_gpu]]
+        res_len = 2 if q.template == "agg" else 4 * q.groups
+        self.res_d[:res_len].zero_()
+        host_res = np.zeros(res_len, np.int32)
+        waves, admitted, left = self._gpu_half(q, gsegs) if gsegs else (0, 0, [])
+        csegs += left
+        c0 = time.perf_counter()
+        if csegs:
+            self._cpu_half(q, csegs, host_res)
+        cpu_ms = (time.perf_counter() - c0) * 1e3
+        out = self.res_h[:res_len]
+        out.copy_(self.res_d[:res_len])  # waits for the GPU share
+        res = merge(q, out.numpy().copy(), host_res)
+        ms = (time.perf_counter() - t0) * 1e3
+        return QueryRun(res, ms, len(cand), self.t.nseg - len(cand), len(gsegs) - len(left), len(csegs), waves,
+                        span, cpu_ms=cpu_ms, admitted=admitted)
+
+    # ---- per-segment timing logs ------------------------------------------------------------
+    def profile_segments(self, q: B.Query, segs: np.ndarray) -> list[dict]:
+        """Time each listed segment of q alone on each device, as the planner would see it:
+        features from the cache state before the segment runs; GPU ms = its column
+        admissions plus one fused launch over it (CUDA events); CPU ms = the CPU engine
+        over it (wall clock, all pool threads). Returns one record per segment."""
+        small = _small_sel(q)
+        self.build_gpu(q)
+        self.build_cpu(q)
+        st = ssb._stream()
+        out = []
+        res_len = 2 if q.template == "agg" else 4 * q.groups
+        host_res = np.zeros(res_len, np.int32)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for sg in segs:
+            sg = int(sg)
+            self.cache.begin_query()
+            ctx = self.context(q, sg, small)
+            f = features(ctx)
+            a_cpu, a_gpu = analytic_ms(ctx)
+            e0.record()
+            try:
+                self._admit(q, sg, st)
+            except L.MbError:
+                continue
+            self._launch_wave(q, [sg], 0)
+            e1.record()
+            e1.synchronize()
+            gpu = e0.elapsed_time(e1)
+            c0 = time.perf_counter()
+            self._cpu_half_nobuild(q, [sg], host_res)
+            cpu_ms = (time.perf_counter() - c0) * 1e3
+            out.append({"features": f, "cpu_ms": cpu_ms, "gpu_ms": gpu, "analytic_cpu_ms": a_cpu,
+                        "analytic_gpu_ms": a_gpu, "template": q.template, "segment": sg,
+                        "resident_frac": ctx.resident_cols / ctx.needed_cols})
+        return out
+
+    def _cpu_half_nobuild(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
+        segs = self._order(np.array(csegs), self.t)
+        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res,
+                      segment_group=segs.astype(np.int16), segment_size=SEG)
+        cpu.star_query(a)
+
+
+def merge(q: B.Query, gpu: np.ndarray, cpu_res: np.ndarray) -> np.ndarray:
+    """Add the CPU share's result into the GPU share's (src/gpudb/CPUProcessing.cu:
+    1786-1819): group keys from whichever side saw the group (the year key, >= 1992,
+    marks a group as seen), 64-bit sums added."""
+    if q.template == "agg":
+        return (gpu.view(np.uint64) + cpu_res.view(np.uint64)).view(np.int32)
+    g = gpu.reshape(-1, 4).copy()
+    c = cpu_res.reshape(-1, 4)
+    seen = c[:, 0] != 0
+    g[seen, :2] = c[seen, :2]
+    sums = g[:, 2:4].copy().view(np.uint64).reshape(-1) + c[:, 2:4].copy().view(np.uint64).reshape(-1)
+    g[:, 2:4] = sums.view(np.int32).reshape(-1, 2)
+    return g.reshape(-1)

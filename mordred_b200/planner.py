@@ -1,0 +1,214 @@
+"""Cost models for placing fact segments on the CPU or the GPU: the reference's analytic
+bandwidth model and the learned MLP, behind one interface.
+
+A planner maps the candidate segments of a query to predicted CPU and GPU milliseconds
+per segment; :func:`place` then splits the segments between the devices to minimise the
+query's makespan (``mb_place_segments``). Features are computed per (query, segment)
+from the query's constants, the segment's min/max statistics and the segment cache's
+residency, the quantities the reference's optimizer reads (segment_min/max,
+CacheManager.h:156-157; selectivities, KernelArgs.h:121-122; residency, segment_bitmap
+CacheManager.h:153; join count; hash-table bytes).
+
+* :class:`AnalyticPlanner` — src/gpudb/CostModel.cu:283-440 restated in C++
+  (``mb_cost_cpu_ms``): CPU cost from 42 GB/s scans and 64-byte line probes; GPU cost
+  zero when resident (CostModel.cu:341-343) plus the 12 GB/s PCIe transfer of the
+  segment's missing columns.
+* :class:`LearnedPlanner` — the 24 -> 64 -> 64 -> 2 MLP of ``mb_mlp_*`` (CUDA forward,
+  backward and Adam) trained on logged per-segment timings; it predicts log CPU ms and
+  log GPU ms. Its weights, feature scaling and training record persist as a small
+  binary file plus a JSON manifest.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import ssb
+
+NUM_FEATURES = L.MB_MLP_IN
+FEATURE_NAMES = [
+    "is_agg", "is_qa", "is_qb", "log2_rows", "date_sel", "discount_sel", "quantity_sel", "s_sel", "c_sel", "p_sel",
+    "log10_sel", "num_probes", "num_filters", "log2_groups", "needed_cols", "resident_frac", "log2_missing_mb",
+    "log2_ht_mb", "log2_out_rows", "agg_op", "log2_cpu_threads", "log_analytic_cpu_ms", "log_analytic_gpu_ms",
+    "cache_free_frac"]
+assert len(FEATURE_NAMES) == NUM_FEATURES
+MIN_MS = 1e-3
+
+
+@dataclass
+class SegmentContext:
+    """What the planners see of one (query, segment): filled by the executor."""
+    template: str
+    rows: int
+    date_sel: float
+    small_sel: dict          # discount, quantity, s, c, p selectivities (1.0 where unconstrained)
+    needed_cols: int
+    resident_cols: int
+    ht_bytes: int
+    groups: int
+    cpu_threads: int
+    cache_free_frac: float
+
+
+def pipeline(ctx: SegmentContext) -> L.MbCostPipeline:
+    """The segment's operator pipeline with its selectivities, for the analytic model."""
+    p = L.MbCostPipeline()
+    s = ctx.small_sel
+    if ctx.template == "agg":
+        fs, ps, aggr = [ctx.date_sel, s["discount"], s["quantity"]], [], 2
+    elif ctx.template == "qa":
+        fs, ps, aggr = [ctx.date_sel], [s["s"], s["p"], 1.0], 1
+    else:
+        fs, ps, aggr = [ctx.date_sel], [s["s"], s["c"], s["p"], 1.0], 2
+    p.num_filters, p.num_probes, p.group_by, p.num_aggr = len(fs), len(ps), 1, aggr
+    for i, v in enumerate(fs):
+        p.filter_sel[i] = v
+    for i, v in enumerate(ps):
+        p.probe_sel[i] = v
+    return p
+
+
+def analytic_ms(ctx: SegmentContext) -> tuple[float, float]:
+    cpu = float(L.lib().mb_cost_cpu_ms(C.byref(pipeline(ctx)), float(ctx.rows)))
+    gpu = float(L.lib().mb_cost_transfer_ms(float(ctx.rows), ctx.needed_cols - ctx.resident_cols))
+    return max(cpu, MIN_MS), max(gpu, MIN_MS)
+
+
+def features(ctx: SegmentContext) -> np.ndarray:
+    s = ctx.small_sel
+    sel = ctx.date_sel * s["discount"] * s["quantity"] * s["s"] * s["c"] * s["p"]
+    nprobe = {"agg": 0, "qa": 3, "qb": 4}[ctx.template]
+    nfilt = {"agg": 3, "qa": 1, "qb": 1}[ctx.template]
+    op = {"agg": L.MB_AGG_MUL, "qa": L.MB_AGG_SUM, "qb": L.MB_AGG_SUB}[ctx.template]
+    missing = (ctx.needed_cols - ctx.resident_cols) * ctx.rows * 4
+    a_cpu, a_gpu = analytic_ms(ctx)
+    return np.array([
+        ctx.template == "agg", ctx.template == "qa", ctx.template == "qb", math.log2(max(ctx.rows, 1)),
+        ctx.date_sel, s["discount"], s["quantity"], s["s"], s["c"], s["p"], math.log10(sel + 1e-7), nprobe, nfilt,
+        math.log2(ctx.groups), ctx.needed_cols, ctx.resident_cols / max(ctx.needed_cols, 1),
+        math.log2(1 + missing / 1e6), math.log2(1 + ctx.ht_bytes / 1e6), math.log2(1 + sel * ctx.rows), op,
+        math.log2(max(ctx.cpu_threads, 1)), math.log(a_cpu), math.log(a_gpu), ctx.cache_free_frac],
+        dtype=np.float32)
+
+
+def place(cpu_ms: np.ndarray, gpu_ms: np.ndarray) -> tuple[np.ndarray, float]:
+    """Split segments between the devices (mb_place_segments): returns (on_gpu, makespan)."""
+    cpu_ms = np.ascontiguousarray(cpu_ms, dtype=np.float64)
+    gpu_ms = np.ascontiguousarray(gpu_ms, dtype=np.float64)
+    on = np.zeros(len(cpu_ms), np.uint8)
+    span = C.c_double(0)
+    L.call("mb_place_segments", len(cpu_ms), cpu_ms.ctypes.data, gpu_ms.ctypes.data, on.ctypes.data, C.byref(span))
+    return on.astype(bool), span.value
+
+
+class AnalyticPlanner:
+    name = "analytic"
+
+    def predict(self, ctxs: list[SegmentContext]) -> tuple[np.ndarray, np.ndarray]:
+        v = np.array([analytic_ms(c) for c in ctxs], dtype=np.float64).reshape(-1, 2)
+        return v[:, 0], v[:, 1]
+
+
+class LearnedPlanner:
+    """The cost MLP on the GPU. `params` is the flat fp32 parameter vector (5,890)."""
+    name = "learned"
+
+    def __init__(self, params: np.ndarray | None = None, mean=None, std=None, seed: int = 0, device="cuda"):
+        self.device = device
+        if params is None:
+            params = init_params(seed)
+        self.params = torch.tensor(np.asarray(params, np.float32), device=device)
+        self.mean = np.zeros(NUM_FEATURES, np.float32) if mean is None else np.asarray(mean, np.float32)
+        self.std = np.ones(NUM_FEATURES, np.float32) if std is None else np.asarray(std, np.float32)
+        self.record: dict = {}
+
+    def _x(self, feats: np.ndarray) -> torch.Tensor:
+        z = (np.asarray(feats, np.float32) - self.mean) / self.std
+        return torch.tensor(z, dtype=torch.float32, device=self.device)
+
+    def predict_log(self, feats: np.ndarray) -> np.ndarray:
+        x = self._x(feats)
+        y = torch.empty(len(feats), 2, dtype=torch.float32, device=self.device)
+        L.call("mb_mlp_forward", self.params.data_ptr(), x.data_ptr(), len(feats), y.data_ptr(), ssb._stream())
+        return y.cpu().numpy().astype(np.float64)
+
+    def predict(self, ctxs: list[SegmentContext]) -> tuple[np.ndarray, np.ndarray]:
+        if not ctxs:
+            return np.zeros(0), np.zeros(0)
+        y = np.exp(self.predict_log(np.stack([features(c) for c in ctxs])))
+        return y[:, 0], y[:, 1]
+
+    def train(self, feats: np.ndarray, log_ms: np.ndarray, epochs: int = 40, batch: int = 256, lr: float = 2e-3,
+              weight_decay: float = 1e-5, seed: int = 0) -> dict:
+        """Fit on (features, [log cpu ms, log gpu ms]) with the CUDA backward and Adam
+        kernels; feature scaling comes from these samples."""
+        feats = np.asarray(feats, np.float32)
+        self.mean = feats.mean(0)
+        self.std = feats.std(0) + 1e-6
+        x = self._x(feats)
+        t = torch.tensor(np.asarray(log_ms, np.float32), device=self.device)
+        n = len(feats)
+        g, m, v = (torch.zeros(L.MB_MLP_PARAMS, dtype=torch.float32, device=self.device) for _ in range(3))
+        loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        rng = np.random.default_rng(seed)
+        st = ssb._stream()
+        step = 0
+        hist = []
+        for ep in range(epochs):
+            perm = torch.tensor(rng.permutation(n), device=self.device)
+            xs, ts = x[perm].contiguous(), t[perm].contiguous()
+            loss.zero_()
+            lr_ep = lr * (0.5 * (1 + math.cos(math.pi * ep / epochs)))  # cosine decay
+            for b0 in range(0, n, batch):
+                nb = min(batch, n - b0)
+                step += 1
+                g.zero_()
+                L.call("mb_mlp_backward", self.params.data_ptr(), xs[b0:].data_ptr(), ts[b0:].data_ptr(), nb,
+                       g.data_ptr(), loss.data_ptr(), st)
+                L.call("mb_mlp_adam", self.params.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
+                       L.MB_MLP_PARAMS, lr_ep, 0.9, 0.999, 1e-8, step, weight_decay, st)
+            hist.append(float(loss.item()) / n)
+        self.record = {"epochs": epochs, "batch": batch, "lr": lr, "steps": step, "samples": n,
+                       "train_loss_per_epoch": hist}
+        return self.record
+
+    def save(self, path_bin: str, manifest: dict | None = None) -> None:
+        os.makedirs(os.path.dirname(path_bin) or ".", exist_ok=True)
+        self.params.cpu().numpy().astype("<f4").tofile(path_bin)
+        man = {"params": os.path.basename(path_bin), "num_params": L.MB_MLP_PARAMS, "layout":
+               "W1[24][64] b1[64] W2[64][64] b2[64] W3[64][2] b3[2], float32 little-endian",
+               "features": FEATURE_NAMES, "feature_mean": self.mean.tolist(), "feature_std": self.std.tolist(),
+               "outputs": ["log_cpu_ms", "log_gpu_ms"], "training": self.record}
+        if manifest:
+            man.update(manifest)
+        with open(os.path.splitext(path_bin)[0] + ".json", "w") as f:
+            json.dump(man, f, indent=1)
+
+    @classmethod
+    def load(cls, path_bin: str, device="cuda") -> "LearnedPlanner":
+        man = json.load(open(os.path.splitext(path_bin)[0] + ".json"))
+        p = np.fromfile(path_bin, dtype="<f4")
+        if p.size != L.MB_MLP_PARAMS:
+            raise ValueError(f"{path_bin}: {p.size} parameters, expected {L.MB_MLP_PARAMS}")
+        out = cls(p, man["feature_mean"], man["feature_std"], device=device)
+        out.record = man.get("training", {})
+        out.manifest = man
+        return out
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-initialised weights, zero biases."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fan_in, fan_out in ((NUM_FEATURES, L.MB_MLP_HIDDEN), (L.MB_MLP_HIDDEN, L.MB_MLP_HIDDEN),
+                            (L.MB_MLP_HIDDEN, L.MB_MLP_OUT)):
+        parts.append(rng.normal(0, math.sqrt(2.0 / fan_in), fan_in * fan_out))
+        parts.append(np.zeros(fan_out))
+    return np.concatenate(parts).astype(np.float32)

@@ -73,6 +73,8 @@ def _stream(stream=None) -> int:
 def _p(t) -> int | None:
     if t is None:
         return None
+    if isinstance(t, int):
+        return t
     if isinstance(t, np.ndarray):
         return t.ctypes.data
     return t.data_ptr()

@@ -1,0 +1,96 @@
+"""Segmented execution: every placement of a query's segments (all GPU, all CPU, the
+planners', random), with a segment cache too small for the query (waves, overflow to the
+CPU), gives the bit-identical result of the whole query on a GPU-resident table."""
+import numpy as np
+import pytest
+import torch
+
+from mordred_b200 import _lib as L
+from mordred_b200 import batch as B
+from mordred_b200 import ssb
+from mordred_b200.engine import SEG, Executor, SegmentedTable
+from mordred_b200.planner import AnalyticPlanner, LearnedPlanner
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    torch.cuda.set_device(0)
+    L.call("mb_init", 0)
+    n = 12 * SEG + 54_321
+    sizes = ssb.Sizes(lo_len=n, s_len=6_000, c_len=80_000, p_len=120_000)
+    t = SegmentedTable(n, 17, sizes)
+    ex = Executor(t, cache_slots=40, policy="lru", max_waves=8)
+    dev = {k: v.cuda() for k, v in t.host_t.items()}
+    return t, ex, dev
+
+
+def _whole(ex, dev, q):
+    """The query over the whole GPU-resident table in one fused launch."""
+    ex.build_gpu(q)
+    res = torch.zeros(2 if q.template == "agg" else 4 * q.groups, dtype=torch.int32, device="cuda")
+    ssb.star_query(ex.args(q, lambda name: dev[name], ex.ht, ex.t.n, res))
+    return res.cpu().numpy()
+
+
+def test_table_is_sorted_and_segment_statistics_hold(setup):
+    t, ex, dev = setup
+    od = t.host["lo_orderdate"]
+    assert (np.diff(od) >= 0).all() and od[0] == 19920101 and od[-1] == 19981231
+    for name in ("lo_revenue", "lo_orderdate"):
+        for sg in (0, 5, t.nseg - 1):
+            seg = t.host[name][sg * SEG: sg * SEG + t.seg_rows[sg]]
+            assert seg.min() == t.min[name][sg] and seg.max() == t.max[name][sg]
+    # every non-date column equals the seeded generator's
+    g = ssb.gen_host(ssb.Sizes(lo_len=t.n, s_len=6_000, c_len=80_000, p_len=120_000), 17, ["lo_custkey"], [])
+    assert np.array_equal(g["lo_custkey"], t.host["lo_custkey"])
+
+
+def test_every_placement_equals_whole_query(setup):
+    t, ex, dev = setup
+    rng = np.random.default_rng(0)
+    qs = B.generate_queries(12, seed=5, sel_lo=1e-3, sel_hi=0.3)
+    learned = LearnedPlanner(seed=1)
+    for q in qs:
+        exp = _whole(ex, dev, q)
+        cand = ex.candidates(q)
+        placements = [np.ones(len(cand), bool), np.zeros(len(cand), bool), rng.random(len(cand)) < 0.5]
+        for on in placements:
+            r = ex.run(q, None, on_gpu=on)
+            assert np.array_equal(r.result, exp), (q.template, on.sum())
+        for planner in (AnalyticPlanner(), learned):
+            r = ex.run(q, planner)
+            assert np.array_equal(r.result, exp), (q.template, planner.name)
+        assert len(cand) < t.nseg or q.date == (19920101, 19981231)
+    assert L.device_status(0) == 0
+
+
+def test_waves_and_overflow_when_cache_is_small(setup):
+    t, ex, dev = setup
+    q = B.Query(template="qb", date=(19920101, 19981231))
+    exp = _whole(ex, dev, q)
+    r = ex.run(q, None, on_gpu=np.ones(t.nseg, bool))  # 13 segments x 6 columns > 40 slots
+    assert r.waves >= 2 and np.array_equal(r.result, exp)
+    st = ex.cache.stats()
+    assert st["resident"] <= 40 and st["evictions"] > 0
+    # profiling records for the planner
+    recs = ex.profile_segments(q, np.array([0, 3, t.nseg - 1]))
+    assert len(recs) == 3 and all(x["gpu_ms"] > 0 and x["cpu_ms"] > 0 for x in recs)
+    assert recs[0]["features"].shape == (24,)
+    assert L.device_status(0) == 0
+
+
+def test_learned_planner_trains_and_round_trips(tmp_path):
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(3)
+    x = rng.normal(0, 1, (5000, 24)).astype(np.float32)
+    y = np.stack([0.5 * x[:, 0] - x[:, 3], np.tanh(x[:, 5]) + 0.2 * x[:, 7]], 1).astype(np.float32)
+    p = LearnedPlanner(seed=0)
+    rec = p.train(x[:4000], y[:4000], epochs=30, batch=256, lr=3e-3)
+    assert rec["train_loss_per_epoch"][-1] < 0.2 * rec["train_loss_per_epoch"][0]
+    pred = p.predict_log(x[4000:])
+    assert np.abs(pred - y[4000:]).mean() < 0.4 * np.abs(y[4000:] - y[4000:].mean(0)).mean()
+    p.save(str(tmp_path / "mlp.bin"), {"note": "test"})
+    q = LearnedPlanner.load(str(tmp_path / "mlp.bin"))
+    assert np.array_equal(q.predict_log(x[:50]), p.predict_log(x[:50]))
