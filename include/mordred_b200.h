@@ -414,12 +414,21 @@ double mb_cost_calculate(const mb_cost_pipeline* pipeline, const int* on_gpu, do
 double mb_cost_cpu_ms(const mb_cost_pipeline* pipeline, double rows);
 /* CostModel.cu:386-390 transfer_cost: `columns` int columns of `rows` rows over PCIe. */
 double mb_cost_transfer_ms(double rows, int columns);
+/* CostModel.cu:427-440 build_cost of a hash-table build over dim_rows rows on the CPU. */
+double mb_cost_build_ms(double dim_rows);
+/* Per-segment analytic estimates for one pipeline: cpu_ms[i] = the all-CPU cost of
+ * rows[i] rows with the first filter's selectivity first_filter_sel[i] (optional);
+ * gpu_ms[i] = the PCIe transfer of the segment's missing_cols[i] columns (optional, 0). */
+int mb_cost_segments(const mb_cost_pipeline* pipeline, int n, const double* rows,
+                     const double* first_filter_sel, const int* missing_cols,
+                     double* cpu_ms, double* gpu_ms);
 /* Split n segments between CPU and GPU (on_gpu[i] = 1: GPU) to minimise
- * max(sum of GPU ms, sum of CPU ms) over a GPU/CPU time-ratio order; *makespan_ms
- * (optional) receives that maximum. No counterpart in the reference, which places by
- * segment residency (QueryOptimizer.cu:1674-1891). */
-int mb_place_segments(int n, const double* cpu_ms, const double* gpu_ms, unsigned char* on_gpu,
-                      double* makespan_ms);
+ * max(cpu_fixed_ms + sum of CPU ms, gpu_fixed_ms + sum of GPU ms) — a device's fixed
+ * cost counts only when it takes a segment — over a GPU/CPU time-ratio order;
+ * *makespan_ms (optional) receives that maximum. No counterpart in the reference, which
+ * places by segment residency (QueryOptimizer.cu:1674-1891). */
+int mb_place_segments(int n, const double* cpu_ms, const double* gpu_ms, double cpu_fixed_ms,
+                      double gpu_fixed_ms, unsigned char* on_gpu, double* makespan_ms);
 
 /* ---- CPU operators (host columns; the CPU half of CPU/GPU split execution) ------- */
 /* Host threads the CPU operators use at most (a persistent pool). */
@@ -483,6 +492,14 @@ int mb_segcache_set_weight(mb_segcache* cache, int col, int seg, double weight);
  * segment pinned by the running query: MB_ERR_SIZE when only those are left). */
 int mb_segcache_admit(mb_segcache* cache, int col, int seg, const int* host_src, int rows,
                       mb_stream_t stream, int* slot_out);
+/* Admit, in order, every listed column of every listed segment (a touch plus
+ * mb_segcache_admit each). host_cols[col] is the host column, seg_rows[seg] the rows of
+ * a segment. *done = segments whose columns are all resident; *copied (optional) +=
+ * column segments copied. MB_ERR_SIZE when segment *done does not fit beside the
+ * pinned segments (some of its columns may have been admitted). */
+int mb_segcache_admit_segments(mb_segcache* cache, const int* cols, int ncols, const int* segs,
+                               int nsegs, const int* const* host_cols, const int* seg_rows,
+                               mb_stream_t stream, int* done, unsigned long long* copied);
 int mb_segcache_evict(mb_segcache* cache, int col, int seg);
 /* Epoch replacement (CacheManager.cu:534-588 SegmentReplacement): weights[col *
  * num_segments + seg] are benefit weights; the positive ones, heaviest first, are made

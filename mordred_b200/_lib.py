@@ -227,7 +227,9 @@ SIGNATURES.update({
     "mb_cost_calculate": (C.c_double, [PS(MbCostPipeline), PS(C.c_int), C.c_double]),
     "mb_cost_cpu_ms": (C.c_double, [PS(MbCostPipeline), C.c_double]),
     "mb_cost_transfer_ms": (C.c_double, [C.c_double, C.c_int]),
-    "mb_place_segments": (I, [I, P, P, P, P]),
+    "mb_place_segments": (I, [I, P, P, C.c_double, C.c_double, P, P]),
+    "mb_cost_build_ms": (C.c_double, [C.c_double]),
+    "mb_cost_segments": (I, [PS(MbCostPipeline), I, P, P, P, P, P]),
     "mb_mlp_forward": (I, [P, P, I, P, P]),
     "mb_mlp_backward": (I, [P, P, P, I, P, P, P]),
     "mb_mlp_adam": (I, [P, P, P, P, I, F32, F32, F32, F32, I, F32, P]),
@@ -249,6 +251,7 @@ SIGNATURES.update({
     "mb_segcache_set_weight": (I, [P, I, I, C.c_double]),
     "mb_segcache_admit": (I, [P, I, I, P, I, P, PS(I)]),
     "mb_segcache_evict": (I, [P, I, I]),
+    "mb_segcache_admit_segments": (I, [P, P, I, P, I, P, P, P, PS(I), PS(C.c_ulonglong)]),
     "mb_segcache_replace": (I, [P, P, P, P, P]),
     "mb_segcache_get_stats": (I, [P, PS(MbSegcacheStats)]),
     "mb_cpu_threads": (I, []),

@@ -16,11 +16,12 @@
 //
 // Placement: given per-segment CPU and GPU time estimates (from this model or from the
 // learned one), segments go to the device where they finish the query soonest. CPU and
-// GPU work on their shares concurrently, so the query takes about max(sum of CPU ms,
-// sum of GPU ms); mb_place_segments orders segments by their GPU/CPU time ratio and
-// picks the split point of that order that minimises this makespan (the optimum for
-// two machines when each segment's times are proportional along the order, and a good
-// heuristic otherwise).
+// GPU work on their shares concurrently, so the query takes about max(fixed CPU ms +
+// sum of CPU ms, fixed GPU ms + sum of GPU ms), a device's fixed cost (its hash-table
+// builds, its launches) paid only when it takes a segment; mb_place_segments orders
+// segments by their GPU/CPU time ratio and picks the split point of that order that
+// minimises this makespan (the optimum for two machines when each segment's times are
+// proportional along the order, and a good heuristic otherwise).
 #include <algorithm>
 #include <cstdint>
 #include <numeric>
@@ -122,13 +123,34 @@ extern "C" double mb_cost_transfer_ms(double rows, int columns) {
   return rows * 4.0 * columns / kBwPci;
 }
 
-extern "C" int mb_place_segments(int n, const double* cpu_ms, const double* gpu_ms, unsigned char* on_gpu,
-                                 double* makespan_ms) {
+extern "C" double mb_cost_build_ms(double dim_rows) {
+  // CostModel.cu:427-440 build_cost without a materialised start: scan + one line per row
+  if (dim_rows < 0) return -1.0;
+  return dim_rows * 4 / kBwCpu + dim_rows * kLine / kBwCpu;
+}
+
+extern "C" int mb_cost_segments(const mb_cost_pipeline* p, int n, const double* rows, const double* first_filter_sel,
+                                const int* missing_cols, double* cpu_ms, double* gpu_ms) {
+  if (!valid(p) || n < 0 || (n > 0 && (rows == nullptr || cpu_ms == nullptr || gpu_ms == nullptr)))
+    return MB_ERR_ARG;
+  mb_cost_pipeline q = *p;
+  for (int i = 0; i < n; ++i) {
+    if (first_filter_sel && q.num_filters > 0) q.filter_sel[0] = first_filter_sel[i];
+    cpu_ms[i] = mb_cost_cpu_ms(&q, rows[i]);
+    gpu_ms[i] = mb_cost_transfer_ms(rows[i], missing_cols ? missing_cols[i] : 0);
+  }
+  return MB_OK;
+}
+
+extern "C" int mb_place_segments(int n, const double* cpu_ms, const double* gpu_ms, double cpu_fixed_ms,
+                                 double gpu_fixed_ms, unsigned char* on_gpu, double* makespan_ms) {
   if (n < 0 || (n > 0 && (cpu_ms == nullptr || gpu_ms == nullptr || on_gpu == nullptr))) return MB_ERR_ARG;
   if (n == 0) {
     if (makespan_ms) *makespan_ms = 0;
     return MB_OK;
   }
+  cpu_fixed_ms = std::max(cpu_fixed_ms, 0.0);
+  gpu_fixed_ms = std::max(gpu_fixed_ms, 0.0);
   std::vector<int> order(n);
   std::iota(order.begin(), order.end(), 0);
   auto ratio = [&](int i) {
@@ -137,13 +159,14 @@ extern "C" int mb_place_segments(int n, const double* cpu_ms, const double* gpu_
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ratio(a) < ratio(b); });
   // GPU takes order[0..k), CPU the rest; k = n .. 0
+  // a device that takes any segment pays its fixed cost (builds, launches) once
   std::vector<double> suffix_cpu(n + 1, 0.0);
   for (int i = n - 1; i >= 0; --i) suffix_cpu[i] = suffix_cpu[i + 1] + std::max(cpu_ms[order[i]], 0.0);
-  double gpu = 0, best = suffix_cpu[0];
+  double gpu = 0, best = suffix_cpu[0] + cpu_fixed_ms;
   int best_k = 0;
   for (int k = 1; k <= n; ++k) {
     gpu += std::max(gpu_ms[order[k - 1]], 0.0);
-    const double span = std::max(gpu, suffix_cpu[k]);
+    const double span = std::max(gpu + gpu_fixed_ms, k < n ? suffix_cpu[k] + cpu_fixed_ms : 0.0);
     if (span < best) {
       best = span;
       best_k = k;

@@ -207,6 +207,38 @@ extern "C" int mb_segcache_admit(mb_segcache* c, int col, int seg, const int* ho
   return MB_OK;
 }
 
+extern "C" int mb_segcache_admit_segments(mb_segcache* c, const int* cols, int ncols, const int* segs, int nsegs,
+                                          const int* const* host_cols, const int* seg_rows, mb_stream_t stream,
+                                          int* done, unsigned long long* copied) {
+  if (c == nullptr || cols == nullptr || segs == nullptr || host_cols == nullptr || seg_rows == nullptr ||
+      ncols < 0 || nsegs < 0 || done == nullptr)
+    return MB_ERR_ARG;
+  *done = 0;
+  for (int i = 0; i < nsegs; ++i) {
+    for (int j = 0; j < ncols; ++j) {
+      const int col = cols[j], seg = segs[i];
+      if (!valid(c, col, seg) || host_cols[col] == nullptr) return MB_ERR_ARG;
+      {
+        std::lock_guard<std::mutex> lk(c->mu);
+        const size_t k = static_cast<size_t>(col) * c->num_segments + seg;
+        ++c->uses[k];
+        if (c->slot_of[k] >= 0)
+          ++c->stats.hits;
+        else
+          ++c->stats.misses;
+      }
+      int slot = -1;
+      const int had = mb_segcache_slot(c, col, seg);
+      const int e = mb_segcache_admit(c, col, seg, host_cols[col] + static_cast<int64_t>(seg) * c->segment_size,
+                                      seg_rows[seg], stream, &slot);
+      if (e != MB_OK) return e;  // MB_ERR_SIZE: segment i does not fit beside the pinned ones
+      if (had < 0 && copied) ++*copied;
+    }
+    *done = i + 1;
+  }
+  return MB_OK;
+}
+
 extern "C" int mb_segcache_evict(mb_segcache* c, int col, int seg) {
   if (!valid(c, col, seg)) return MB_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);

@@ -22,9 +22,6 @@ library's operators:
 """
 from __future__ import annotations
 
-import ctypes as C
-import math
-import threading
 import time
 from dataclasses import dataclass, field
 
@@ -34,7 +31,7 @@ import torch
 from . import _lib as L
 from . import batch as B
 from . import cpu, ssb
-from .planner import SegmentContext, features, place, analytic_ms
+from .planner import QueryContext, analytic_ms, features, place
 from .segcache import SegmentCache
 
 SEG = 1 << 20
@@ -159,8 +156,7 @@ class Executor:
         self.res_d = torch.zeros(4 * ssb.QA_GROUPS, dtype=torch.int32, device="cuda")
         self.res_h = torch.empty(4 * ssb.QA_GROUPS, dtype=torch.int32, pin_memory=True)
         self.cpu_threads = cpu.threads()
-        # the day-0 date key of the table's date dimension (for the date probe's slots)
-        self.date_slots = ssb.DATE_SLOTS
+        self._host_ptrs = [table.ptr(c, 0) if c in table.host else None for c in FACT]
 
     # ---- planning inputs ----------------------------------------------------------------
     def candidates(self, q: B.Query) -> np.ndarray:
@@ -174,20 +170,28 @@ class Executor:
                     ok &= (t.max[name] >= r[0]) & (t.min[name] <= r[1])
         return np.nonzero(ok)[0]
 
-    def context(self, q: B.Query, seg: int, small: dict) -> SegmentContext:
+    def context(self, q: B.Query, segs: np.ndarray) -> QueryContext:
+        """The planners' view of q over `segs`: rows, in-range share of each segment's
+        rows (the table is date-sorted, so a segment's dates are contiguous), residency of
+        the needed columns, hash-table sizes."""
         t = self.t
-        lo, hi = t.seg_day_lo[seg], t.seg_day_hi[seg]
+        segs = np.asarray(segs, np.int64)
+        lo, hi = t.seg_day_lo[segs], t.seg_day_hi[segs]
         qlo, qhi = _day(q.date[0]), _day(q.date[1] + 1) - 1
-        inter = max(0, min(hi, qhi) - max(lo, qlo) + 1)
-        date_sel = inter / max(1, hi - lo + 1)
+        inter = np.maximum(0, np.minimum(hi, qhi) - np.maximum(lo, qlo) + 1)
+        date_sel = inter / np.maximum(1, hi - lo + 1)
         need = NEEDED[q.template]
-        res = sum(self.cache.slot(COL_ID[c], int(seg)) >= 0 for c in need)
+        res = np.zeros(len(segs), np.int32)
+        for c in need:
+            res += self.cache.col_idx(COL_ID[c])[segs] >= 0
         s = t.sizes
         ht_bytes = {"agg": 0, "qa": 4 * (s.s_len + 2 * s.p_len + 2 * ssb.DATE_SLOTS),
                     "qb": 4 * (s.s_len + 2 * s.c_len + s.p_len + 2 * ssb.DATE_SLOTS)}[q.template]
+        dim_rows = {"agg": 0, "qa": s.s_len + s.p_len + s.d_len, "qb": s.s_len + s.c_len + s.p_len + s.d_len}
         free = 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
-        return SegmentContext(q.template, int(t.seg_rows[seg]), float(date_sel), small, len(need), int(res),
-                              ht_bytes, q.groups, self.cpu_threads, free)
+        return QueryContext(q.template, t.seg_rows[segs].astype(np.float64), date_sel.astype(np.float64),
+                            _small_sel(q), len(need), res, ht_bytes, dim_rows[q.template], q.groups,
+                            self.cpu_threads, free)
 
     # ---- builds ------------------------------------------------------------------------
     def build_gpu(self, q: B.Query) -> None:
@@ -288,58 +292,37 @@ class Executor:
                       segment_group=self.seg_d[w], segment_size=SEG)
         ssb.star_query(a)
 
-    def _admit(self, q: B.Query, seg: int, st: int) -> int:
-        """Make the query's columns of `seg` resident (pinned for the running query);
-        returns the column segments copied. Raises MbError(MB_ERR_SIZE) when the cache
-        is full of pinned segments."""
-        n = 0
-        for c in (COL_ID[x] for x in NEEDED[q.template]):
-            self.cache.touch(c, seg)
-            if self.cache.slot(c, seg) < 0:
-                self.cache.admit(c, seg, self.t.ptr(FACT[c], seg), int(self.t.seg_rows[seg]), st)
-                n += 1
-        return n
+    def _admit(self, q: B.Query, segs: list[int], st: int) -> tuple[int, int]:
+        """Make the query's columns of `segs` resident, in order (pinned for the running
+        query); returns (segments admitted, column segments copied)."""
+        cols = [COL_ID[x] for x in NEEDED[q.template]]
+        return self.cache.admit_segments(cols, segs, self._host_ptrs, self.t.seg_rows, st)
 
     def _gpu_half(self, q: B.Query, gsegs: list[int]) -> tuple[int, int, list[int]]:
         """Enqueue the GPU share on the current stream: builds, admissions, one fused
         launch per wave. Returns (waves, column segments admitted, segments left over)."""
         st = ssb._stream()
         self.build_gpu(q)
-        waves: list[list[int]] = [[]]
+        waves = 0
         admitted = 0
-        left: list[int] = []
-        for sgi in gsegs:
-            try:
-                admitted += self._admit(q, sgi, st)
-                waves[-1].append(sgi)
-                continue
-            except L.MbError as e:
-                if e.code != L.MB_ERR_SIZE or not waves[-1] or len(waves) == self.max_waves:
-                    left.append(sgi)
-                    continue
-            # the cache is full of this wave's segments: launch it, then unpin it so the next
-            # wave may recycle its slots (copies into them are ordered after its kernel on
-            # this stream)
-            self._launch_wave(q, waves[-1], len(waves) - 1)
-            waves.append([])
-            self.cache.begin_query()
-            try:
-                admitted += self._admit(q, sgi, st)
-                waves[-1].append(sgi)
-            except L.MbError:
-                left.append(sgi)
-        if waves[-1]:
-            self._launch_wave(q, waves[-1], len(waves) - 1)
-        else:
-            waves.pop()
-        return len(waves), admitted, left
+        rest = list(gsegs)
+        while rest and waves < self.max_waves:
+            done, copied = self._admit(q, rest, st)
+            admitted += copied
+            if done == 0:
+                break  # not even one segment fits: the CPU takes the rest
+            # launch the wave, then unpin it so the next wave may recycle its slots (copies
+            # into them are ordered after its kernel on this stream)
+            self._launch_wave(q, rest[:done], waves)
+            waves += 1
+            rest = rest[done:]
+            if rest:
+                self.cache.begin_query()
+        return waves, admitted, rest
 
     def _cpu_half(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
         self.build_cpu(q)
-        segs = self._order(np.array(csegs), self.t)
-        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res,
-                      segment_group=segs.astype(np.int16), segment_size=SEG)
-        cpu.star_query(a)
+        self._cpu_segments(q, csegs, res)
 
     # ---- one query -----------------------------------------------------------------------
     def run(self, q: B.Query, planner, on_gpu: np.ndarray | None = None) -> QueryRun:
@@ -349,13 +332,11 @@ class Executor:
         works; the CPU also takes GPU segments the cache could not hold."""
         t0 = time.perf_counter()
         cand = self.candidates(q)
-        small = _small_sel(q)
         self.cache.begin_query()
         span = float("nan")
         if on_gpu is None:
-            ctxs = [self.context(q, int(s), small) for s in cand]
-            pc, pg = planner.predict(ctxs)
-            on_gpu, span = place(pc, pg)
+            pc, pg, fc, fg = planner.predict(self.context(q, cand))
+            on_gpu, span = place(pc, pg, fc, fg)
         gsegs = [int(s) for s in cand[on_gpu]]
         csegs = [int(s) for s in cand[~on_gpu]]
         res_len = 2 if q.template == "agg" else 4 * q.groups
@@ -375,43 +356,80 @@ class Executor:
                         span, cpu_ms=cpu_ms, admitted=admitted)
 
     # ---- per-segment timing logs ------------------------------------------------------------
-    def profile_segments(self, q: B.Query, segs: np.ndarray) -> list[dict]:
-        """Time each listed segment of q alone on each device, as the planner would see it:
-        features from the cache state before the segment runs; GPU ms = its column
-        admissions plus one fused launch over it (CUDA events); CPU ms = the CPU engine
-        over it (wall clock, all pool threads). Returns one record per segment."""
-        small = _small_sel(q)
-        self.build_gpu(q)
-        self.build_cpu(q)
+    def profile_segments(self, q: B.Query, segs: np.ndarray) -> tuple[list[dict], dict]:
+        """Per-segment costs of q on each device, as the planner should see them.
+
+        Each listed segment runs alone on each device (CUDA events around its column
+        admissions and around one fused launch over it; wall clock around the CPU engine
+        over it); then all of them run together in one launch and one CPU call. A
+        segment's logged cost is its share of the batched time (in proportion to its
+        solo time) plus, on the GPU, its own admission copies: the marginal cost it adds
+        to a query's share, without the per-call overheads a solo run pays. Features come
+        from the cache state before the segment's admission. Also returns the query's
+        fixed costs: hash-table builds on each device."""
         st = ssb._stream()
-        out = []
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record()
+        self.build_gpu(q)
+        e[1].record()
+        e[1].synchronize()
+        gpu_build = e[0].elapsed_time(e[1])
+        c0 = time.perf_counter()
+        self.build_cpu(q)
+        cpu_build = (time.perf_counter() - c0) * 1e3
         res_len = 2 if q.template == "agg" else 4 * q.groups
         host_res = np.zeros(res_len, np.int32)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.cache.begin_query()
+        segs = [int(x) for x in segs]
+        # keep the partial last segment, if listed, for the end (segment lists put it last)
+        segs = [int(x) for x in self._order(np.array(segs), self.t)]
+        ctx = self.context(q, np.array(segs))
+        feats = features(ctx)
+        a_cpu, a_gpu = analytic_ms(ctx)
+        xfer, ksolo, csolo, ok = [], [], [], []
         for sg in segs:
-            sg = int(sg)
-            self.cache.begin_query()
-            ctx = self.context(q, sg, small)
-            f = features(ctx)
-            a_cpu, a_gpu = analytic_ms(ctx)
-            e0.record()
-            try:
-                self._admit(q, sg, st)
-            except L.MbError:
+            e[0].record()
+            done, _ = self._admit(q, [sg], st)
+            e[1].record()
+            if done == 0:
+                ok.append(False)
+                xfer.append(0.0), ksolo.append(0.0), csolo.append(0.0)
                 continue
             self._launch_wave(q, [sg], 0)
-            e1.record()
-            e1.synchronize()
-            gpu = e0.elapsed_time(e1)
+            e[2].record()
+            e[2].synchronize()
+            xfer.append(e[0].elapsed_time(e[1]))
+            ksolo.append(e[1].elapsed_time(e[2]))
             c0 = time.perf_counter()
-            self._cpu_half_nobuild(q, [sg], host_res)
-            cpu_ms = (time.perf_counter() - c0) * 1e3
-            out.append({"features": f, "cpu_ms": cpu_ms, "gpu_ms": gpu, "analytic_cpu_ms": a_cpu,
-                        "analytic_gpu_ms": a_gpu, "template": q.template, "segment": sg,
-                        "resident_frac": ctx.resident_cols / ctx.needed_cols})
-        return out
+            self._cpu_segments(q, [sg], host_res)
+            csolo.append((time.perf_counter() - c0) * 1e3)
+            ok.append(True)
+        okseg = [sg for sg, k in zip(segs, ok) if k]
+        if not okseg:
+            return [], {"template": q.template, "cpu_build_ms": cpu_build, "gpu_build_ms": gpu_build}
+        e[0].record()
+        self._launch_wave(q, okseg, 1)
+        e[1].record()
+        e[1].synchronize()
+        kbatch = e[0].elapsed_time(e[1])
+        c0 = time.perf_counter()
+        self._cpu_segments(q, okseg, host_res)
+        cbatch = (time.perf_counter() - c0) * 1e3
+        ks = sum(k for k, o in zip(ksolo, ok) if o)
+        cs = sum(c for c, o in zip(csolo, ok) if o)
+        out = []
+        for i, sg in enumerate(segs):
+            if not ok[i]:
+                continue
+            out.append({"features": feats[i], "cpu_ms": cbatch * csolo[i] / cs,
+                        "gpu_ms": xfer[i] + kbatch * ksolo[i] / ks, "cpu_solo_ms": csolo[i],
+                        "gpu_solo_ms": xfer[i] + ksolo[i], "analytic_cpu_ms": float(a_cpu[i]),
+                        "analytic_gpu_ms": float(a_gpu[i]), "template": q.template, "segment": sg,
+                        "resident_frac": float(ctx.resident_cols[i]) / ctx.needed_cols})
+        return out, {"template": q.template, "cpu_build_ms": cpu_build, "gpu_build_ms": gpu_build,
+                     "segments": len(okseg), "gpu_batch_kernel_ms": kbatch, "cpu_batch_ms": cbatch}
 
-    def _cpu_half_nobuild(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
+    def _cpu_segments(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
         segs = self._order(np.array(csegs), self.t)
         a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res,
                       segment_group=segs.astype(np.int16), segment_size=SEG)

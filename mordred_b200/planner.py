@@ -2,21 +2,24 @@
 bandwidth model and the learned MLP, behind one interface.
 
 A planner maps the candidate segments of a query to predicted CPU and GPU milliseconds
-per segment; :func:`place` then splits the segments between the devices to minimise the
-query's makespan (``mb_place_segments``). Features are computed per (query, segment)
-from the query's constants, the segment's min/max statistics and the segment cache's
-residency, the quantities the reference's optimizer reads (segment_min/max,
-CacheManager.h:156-157; selectivities, KernelArgs.h:121-122; residency, segment_bitmap
-CacheManager.h:153; join count; hash-table bytes).
+per segment, plus each device's fixed cost for the query (its hash-table builds and
+launches, paid once if the device takes any segment); :func:`place` then splits the
+segments between the devices to minimise the query's makespan
+(``mb_place_segments``). Features are computed per (query, segment) from the query's
+constants, the segment's min/max statistics and the segment cache's residency, the
+quantities the reference's optimizer reads (segment_min/max, CacheManager.h:156-157;
+selectivities, KernelArgs.h:121-122; residency, segment_bitmap CacheManager.h:153; join
+count; hash-table bytes).
 
 * :class:`AnalyticPlanner` — src/gpudb/CostModel.cu:283-440 restated in C++
-  (``mb_cost_cpu_ms``): CPU cost from 42 GB/s scans and 64-byte line probes; GPU cost
-  zero when resident (CostModel.cu:341-343) plus the 12 GB/s PCIe transfer of the
-  segment's missing columns.
+  (``mb_cost_segments``, ``mb_cost_build_ms``): CPU cost from 42 GB/s scans and 64-byte
+  line probes, plus the CPU hash-table builds; GPU cost zero when resident
+  (CostModel.cu:341-343) plus the 12 GB/s PCIe transfer of the segment's missing columns.
 * :class:`LearnedPlanner` — the 24 -> 64 -> 64 -> 2 MLP of ``mb_mlp_*`` (CUDA forward,
   backward and Adam) trained on logged per-segment timings; it predicts log CPU ms and
-  log GPU ms. Its weights, feature scaling and training record persist as a small
-  binary file plus a JSON manifest.
+  log GPU ms per segment; its fixed costs per query form are the logged medians. Its
+  weights, feature scaling, fixed costs and training record persist as a small binary
+  file plus a JSON manifest.
 """
 from __future__ import annotations
 
@@ -40,33 +43,43 @@ FEATURE_NAMES = [
     "cache_free_frac"]
 assert len(FEATURE_NAMES) == NUM_FEATURES
 MIN_MS = 1e-3
+TEMPLATES = ("agg", "qa", "qb")
 
 
 @dataclass
-class SegmentContext:
-    """What the planners see of one (query, segment): filled by the executor."""
+class QueryContext:
+    """What the planners see of a query's candidate segments (arrays over segments)."""
     template: str
-    rows: int
-    date_sel: float
-    small_sel: dict          # discount, quantity, s, c, p selectivities (1.0 where unconstrained)
+    rows: np.ndarray           # float64
+    date_sel: np.ndarray       # share of each segment's rows inside the query's date range
+    small_sel: dict            # discount, quantity, s, c, p selectivities (1.0 where unconstrained)
     needed_cols: int
-    resident_cols: int
+    resident_cols: np.ndarray  # int32, needed columns resident per segment
     ht_bytes: int
+    dim_rows: int              # dimension rows the query's hash-table builds scan
     groups: int
     cpu_threads: int
     cache_free_frac: float
 
+    def __len__(self) -> int:
+        return len(self.rows)
 
-def pipeline(ctx: SegmentContext) -> L.MbCostPipeline:
-    """The segment's operator pipeline with its selectivities, for the analytic model."""
+    def subset(self, idx) -> "QueryContext":
+        return QueryContext(self.template, self.rows[idx], self.date_sel[idx], self.small_sel, self.needed_cols,
+                            self.resident_cols[idx], self.ht_bytes, self.dim_rows, self.groups, self.cpu_threads,
+                            self.cache_free_frac)
+
+
+def pipeline(ctx: QueryContext) -> L.MbCostPipeline:
+    """The query's operator pipeline (the date filter first) for the analytic model."""
     p = L.MbCostPipeline()
     s = ctx.small_sel
     if ctx.template == "agg":
-        fs, ps, aggr = [ctx.date_sel, s["discount"], s["quantity"]], [], 2
+        fs, ps, aggr = [1.0, s["discount"], s["quantity"]], [], 2
     elif ctx.template == "qa":
-        fs, ps, aggr = [ctx.date_sel], [s["s"], s["p"], 1.0], 1
+        fs, ps, aggr = [1.0], [s["s"], s["p"], 1.0], 1
     else:
-        fs, ps, aggr = [ctx.date_sel], [s["s"], s["c"], s["p"], 1.0], 2
+        fs, ps, aggr = [1.0], [s["s"], s["c"], s["p"], 1.0], 2
     p.num_filters, p.num_probes, p.group_by, p.num_aggr = len(fs), len(ps), 1, aggr
     for i, v in enumerate(fs):
         p.filter_sel[i] = v
@@ -75,59 +88,83 @@ def pipeline(ctx: SegmentContext) -> L.MbCostPipeline:
     return p
 
 
-def analytic_ms(ctx: SegmentContext) -> tuple[float, float]:
-    cpu = float(L.lib().mb_cost_cpu_ms(C.byref(pipeline(ctx)), float(ctx.rows)))
-    gpu = float(L.lib().mb_cost_transfer_ms(float(ctx.rows), ctx.needed_cols - ctx.resident_cols))
-    return max(cpu, MIN_MS), max(gpu, MIN_MS)
+def analytic_ms(ctx: QueryContext) -> tuple[np.ndarray, np.ndarray]:
+    n = len(ctx)
+    cpu, gpu = np.zeros(n), np.zeros(n)
+    rows = np.ascontiguousarray(ctx.rows, dtype=np.float64)
+    sel = np.ascontiguousarray(ctx.date_sel, dtype=np.float64)
+    miss = np.ascontiguousarray(ctx.needed_cols - ctx.resident_cols, dtype=np.int32)
+    L.call("mb_cost_segments", C.byref(pipeline(ctx)), n, rows.ctypes.data, sel.ctypes.data, miss.ctypes.data,
+           cpu.ctypes.data, gpu.ctypes.data)
+    return np.maximum(cpu, MIN_MS), np.maximum(gpu, MIN_MS)
 
 
-def features(ctx: SegmentContext) -> np.ndarray:
+def features(ctx: QueryContext) -> np.ndarray:
+    n = len(ctx)
     s = ctx.small_sel
-    sel = ctx.date_sel * s["discount"] * s["quantity"] * s["s"] * s["c"] * s["p"]
+    small = s["discount"] * s["quantity"] * s["s"] * s["c"] * s["p"]
+    sel = ctx.date_sel * small
     nprobe = {"agg": 0, "qa": 3, "qb": 4}[ctx.template]
     nfilt = {"agg": 3, "qa": 1, "qb": 1}[ctx.template]
     op = {"agg": L.MB_AGG_MUL, "qa": L.MB_AGG_SUM, "qb": L.MB_AGG_SUB}[ctx.template]
     missing = (ctx.needed_cols - ctx.resident_cols) * ctx.rows * 4
     a_cpu, a_gpu = analytic_ms(ctx)
-    return np.array([
-        ctx.template == "agg", ctx.template == "qa", ctx.template == "qb", math.log2(max(ctx.rows, 1)),
-        ctx.date_sel, s["discount"], s["quantity"], s["s"], s["c"], s["p"], math.log10(sel + 1e-7), nprobe, nfilt,
-        math.log2(ctx.groups), ctx.needed_cols, ctx.resident_cols / max(ctx.needed_cols, 1),
-        math.log2(1 + missing / 1e6), math.log2(1 + ctx.ht_bytes / 1e6), math.log2(1 + sel * ctx.rows), op,
-        math.log2(max(ctx.cpu_threads, 1)), math.log(a_cpu), math.log(a_gpu), ctx.cache_free_frac],
-        dtype=np.float32)
+    f = np.empty((n, NUM_FEATURES), np.float32)
+    const = [ctx.template == "agg", ctx.template == "qa", ctx.template == "qb"]
+    f[:, 0:3] = np.array(const, np.float32)
+    f[:, 3] = np.log2(np.maximum(ctx.rows, 1))
+    f[:, 4] = ctx.date_sel
+    f[:, 5:10] = [s["discount"], s["quantity"], s["s"], s["c"], s["p"]]
+    f[:, 10] = np.log10(sel + 1e-7)
+    f[:, 11], f[:, 12] = nprobe, nfilt
+    f[:, 13] = math.log2(ctx.groups)
+    f[:, 14] = ctx.needed_cols
+    f[:, 15] = ctx.resident_cols / max(ctx.needed_cols, 1)
+    f[:, 16] = np.log2(1 + missing / 1e6)
+    f[:, 17] = math.log2(1 + ctx.ht_bytes / 1e6)
+    f[:, 18] = np.log2(1 + sel * ctx.rows)
+    f[:, 19] = op
+    f[:, 20] = math.log2(max(ctx.cpu_threads, 1))
+    f[:, 21] = np.log(a_cpu)
+    f[:, 22] = np.log(a_gpu)
+    f[:, 23] = ctx.cache_free_frac
+    return f
 
 
-def place(cpu_ms: np.ndarray, gpu_ms: np.ndarray) -> tuple[np.ndarray, float]:
+def place(cpu_ms: np.ndarray, gpu_ms: np.ndarray, cpu_fixed: float = 0.0, gpu_fixed: float = 0.0):
     """Split segments between the devices (mb_place_segments): returns (on_gpu, makespan)."""
     cpu_ms = np.ascontiguousarray(cpu_ms, dtype=np.float64)
     gpu_ms = np.ascontiguousarray(gpu_ms, dtype=np.float64)
     on = np.zeros(len(cpu_ms), np.uint8)
     span = C.c_double(0)
-    L.call("mb_place_segments", len(cpu_ms), cpu_ms.ctypes.data, gpu_ms.ctypes.data, on.ctypes.data, C.byref(span))
+    L.call("mb_place_segments", len(cpu_ms), cpu_ms.ctypes.data, gpu_ms.ctypes.data, float(cpu_fixed),
+           float(gpu_fixed), on.ctypes.data, C.byref(span))
     return on.astype(bool), span.value
 
 
 class AnalyticPlanner:
     name = "analytic"
 
-    def predict(self, ctxs: list[SegmentContext]) -> tuple[np.ndarray, np.ndarray]:
-        v = np.array([analytic_ms(c) for c in ctxs], dtype=np.float64).reshape(-1, 2)
-        return v[:, 0], v[:, 1]
+    def predict(self, ctx: QueryContext):
+        cpu, gpu = analytic_ms(ctx)
+        return cpu, gpu, float(L.lib().mb_cost_build_ms(float(ctx.dim_rows))), 0.0
 
 
 class LearnedPlanner:
     """The cost MLP on the GPU. `params` is the flat fp32 parameter vector (5,890)."""
     name = "learned"
 
-    def __init__(self, params: np.ndarray | None = None, mean=None, std=None, seed: int = 0, device="cuda"):
+    def __init__(self, params: np.ndarray | None = None, mean=None, std=None, seed: int = 0, device="cuda",
+                 fixed_ms: dict | None = None):
         self.device = device
         if params is None:
             params = init_params(seed)
         self.params = torch.tensor(np.asarray(params, np.float32), device=device)
         self.mean = np.zeros(NUM_FEATURES, np.float32) if mean is None else np.asarray(mean, np.float32)
         self.std = np.ones(NUM_FEATURES, np.float32) if std is None else np.asarray(std, np.float32)
+        self.fixed_ms = fixed_ms or {t: [0.0, 0.0] for t in TEMPLATES}
         self.record: dict = {}
+        self.manifest: dict = {}
 
     def _x(self, feats: np.ndarray) -> torch.Tensor:
         z = (np.asarray(feats, np.float32) - self.mean) / self.std
@@ -139,11 +176,12 @@ class LearnedPlanner:
         L.call("mb_mlp_forward", self.params.data_ptr(), x.data_ptr(), len(feats), y.data_ptr(), ssb._stream())
         return y.cpu().numpy().astype(np.float64)
 
-    def predict(self, ctxs: list[SegmentContext]) -> tuple[np.ndarray, np.ndarray]:
-        if not ctxs:
-            return np.zeros(0), np.zeros(0)
-        y = np.exp(self.predict_log(np.stack([features(c) for c in ctxs])))
-        return y[:, 0], y[:, 1]
+    def predict(self, ctx: QueryContext):
+        fc, fg = self.fixed_ms.get(ctx.template, [0.0, 0.0])
+        if len(ctx) == 0:
+            return np.zeros(0), np.zeros(0), fc, fg
+        y = np.exp(self.predict_log(features(ctx)))
+        return y[:, 0], y[:, 1], fc, fg
 
     def train(self, feats: np.ndarray, log_ms: np.ndarray, epochs: int = 40, batch: int = 256, lr: float = 2e-3,
               weight_decay: float = 1e-5, seed: int = 0) -> dict:
@@ -185,7 +223,7 @@ class LearnedPlanner:
         man = {"params": os.path.basename(path_bin), "num_params": L.MB_MLP_PARAMS, "layout":
                "W1[24][64] b1[64] W2[64][64] b2[64] W3[64][2] b3[2], float32 little-endian",
                "features": FEATURE_NAMES, "feature_mean": self.mean.tolist(), "feature_std": self.std.tolist(),
-               "outputs": ["log_cpu_ms", "log_gpu_ms"], "training": self.record}
+               "outputs": ["log_cpu_ms", "log_gpu_ms"], "fixed_ms": self.fixed_ms, "training": self.record}
         if manifest:
             man.update(manifest)
         with open(os.path.splitext(path_bin)[0] + ".json", "w") as f:
@@ -197,7 +235,7 @@ class LearnedPlanner:
         p = np.fromfile(path_bin, dtype="<f4")
         if p.size != L.MB_MLP_PARAMS:
             raise ValueError(f"{path_bin}: {p.size} parameters, expected {L.MB_MLP_PARAMS}")
-        out = cls(p, man["feature_mean"], man["feature_std"], device=device)
+        out = cls(p, man["feature_mean"], man["feature_std"], device=device, fixed_ms=man.get("fixed_ms"))
         out.record = man.get("training", {})
         out.manifest = man
         return out

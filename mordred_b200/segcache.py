@@ -60,6 +60,21 @@ class SegmentCache:
         L.call("mb_segcache_admit", self.h, col, seg, host_ptr, rows, stream, C.byref(slot))
         return slot.value
 
+    def admit_segments(self, cols, segs, host_cols: list, seg_rows: np.ndarray, stream: int = 0) -> tuple[int, int]:
+        """Admit every column in `cols` of every segment in `segs`, in order; returns
+        (segments fully admitted, column segments copied). Stops at the first segment that
+        does not fit beside the pinned ones."""
+        cols = np.ascontiguousarray(cols, dtype=np.int32)
+        segs = np.ascontiguousarray(segs, dtype=np.int32)
+        ptrs = (C.c_void_p * self.num_columns)(*host_cols)
+        rows = np.ascontiguousarray(seg_rows, dtype=np.int32)
+        done, copied = C.c_int(0), C.c_ulonglong(0)
+        code = L.lib().mb_segcache_admit_segments(self.h, cols.ctypes.data, len(cols), segs.ctypes.data, len(segs),
+                                                  ptrs, rows.ctypes.data, stream, C.byref(done), C.byref(copied))
+        if code not in (L.MB_OK, L.MB_ERR_SIZE):
+            L.check("mb_segcache_admit_segments", code)
+        return done.value, int(copied.value)
+
     def evict(self, col: int, seg: int) -> None:
         L.call("mb_segcache_evict", self.h, col, seg)
 

@@ -20,6 +20,20 @@ def _pipe(fs, ps, group_by=1, n_aggr=2):
     return p
 
 
+def test_segment_batch_and_build_cost():
+    p = _pipe([0.5, 0.3], [0.2, 1.0], 1, 2)
+    rows = np.array([1e6, 5e5, 1048576.0])
+    sel = np.array([0.1, 1.0, 0.0])
+    miss = np.array([0, 3, 6], np.int32)
+    cpu_ms, gpu_ms = np.zeros(3), np.zeros(3)
+    L.call("mb_cost_segments", C.byref(p), 3, rows.ctypes.data, sel.ctypes.data, miss.ctypes.data, cpu_ms.ctypes.data,
+           gpu_ms.ctypes.data)
+    for i in range(3):
+        assert abs(cpu_ms[i] - CO.calculate_cost([sel[i], 0.3], [0.2, 1.0], 1, 2, [0] * 5, rows[i])) < 1e-12
+        assert abs(gpu_ms[i] - rows[i] * 4 * miss[i] / 12e6) < 1e-12
+    assert abs(L.lib().mb_cost_build_ms(1e6) - (1e6 * 4 + 1e6 * 64) / 42e6) < 1e-12
+
+
 def test_hand_computed_all_cpu():
     # 1e6 rows: filter 0.3 keeps 3e5; probe 0.2 keeps 6e4; group over 2 aggregate columns
     p = _pipe([0.3], [0.2])
@@ -43,20 +57,30 @@ def test_every_placement_matches_restatement():
             assert abs(got - exp) <= 1e-9 * max(1.0, abs(exp)), (fs, ps, g, dev)
 
 
+def _span(cpu, gpu, on, cf, gf):
+    g = gpu[on].sum() + (gf if on.any() else 0.0)
+    c = cpu[~on].sum() + (cf if (~on).any() else 0.0)
+    return max(g, c)
+
+
 @pytest.mark.parametrize("n", [0, 1, 2, 7, 40])
-def test_placement_is_best_split_of_ratio_order(n):
+@pytest.mark.parametrize("fixed", [(0.0, 0.0), (2.0, 0.3)])
+def test_placement_is_best_split_of_ratio_order(n, fixed):
+    cf, gf = fixed
     rng = np.random.default_rng(n)
     cpu = rng.uniform(0.1, 5, n)
     gpu = rng.uniform(0.0, 3, n)
     on = np.zeros(n, np.uint8)
     span = C.c_double(0)
-    L.call("mb_place_segments", n, cpu.ctypes.data, gpu.ctypes.data, on.ctypes.data, C.byref(span))
-    got = max(gpu[on == 1].sum(), cpu[on == 0].sum()) if n else 0.0
+    L.call("mb_place_segments", n, cpu.ctypes.data, gpu.ctypes.data, cf, gf, on.ctypes.data, C.byref(span))
+    on = on.astype(bool)
+    got = _span(cpu, gpu, on, cf, gf) if n else 0.0
     assert abs(got - span.value) < 1e-9
     order = np.argsort(gpu / cpu, kind="stable")
-    best = min(max(gpu[order[:k]].sum(), cpu[order[k:]].sum()) for k in range(n + 1)) if n else 0.0
+    best = 0.0
+    if n:
+        best = min(_span(cpu, gpu, np.isin(np.arange(n), order[:k]), cf, gf) for k in range(n + 1))
     assert abs(span.value - best) < 1e-9
     if n <= 10 and n > 0:  # and near the true optimum over all 2^n assignments
-        opt = min(max(gpu[np.array(m, bool)].sum(), cpu[~np.array(m, bool)].sum())
-                  for m in itertools.product([0, 1], repeat=n))
+        opt = min(_span(cpu, gpu, np.array(m, bool), cf, gf) for m in itertools.product([0, 1], repeat=n))
         assert span.value <= opt + max(gpu.max(), cpu.max())

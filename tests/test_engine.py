@@ -75,9 +75,11 @@ def test_waves_and_overflow_when_cache_is_small(setup):
     st = ex.cache.stats()
     assert st["resident"] <= 40 and st["evictions"] > 0
     # profiling records for the planner
-    recs = ex.profile_segments(q, np.array([0, 3, t.nseg - 1]))
+    recs, fixed = ex.profile_segments(q, np.array([t.nseg - 1, 0, 3]))
     assert len(recs) == 3 and all(x["gpu_ms"] > 0 and x["cpu_ms"] > 0 for x in recs)
-    assert recs[0]["features"].shape == (24,)
+    assert recs[0]["features"].shape == (24,) and recs[-1]["segment"] == t.nseg - 1
+    assert sum(x["cpu_ms"] for x in recs) == pytest.approx(fixed["cpu_batch_ms"])
+    assert fixed["cpu_build_ms"] > 0 and fixed["gpu_build_ms"] > 0
     assert L.device_status(0) == 0
 
 

@@ -84,3 +84,18 @@ def test_bad_arguments():
     c = SegmentCache(1, SEG, 1, 2, device=-1)
     with pytest.raises(L.MbError):
         c.touch(1, 0)
+
+
+def test_admit_segments_in_order_until_full():
+    cols = _cols(3, 6)
+    c = SegmentCache(7, SEG, 3, 6, "lru", device=-1)
+    rows = np.full(6, SEG, np.int32)
+    c.begin_query()
+    done, copied = c.admit_segments([0, 2], [4, 1, 5, 0], [x.ctypes.data for x in cols], rows)
+    assert done == 3 and copied == 7  # the fourth segment gets one column in; the second does not fit
+    for seg in (4, 1, 5):
+        for col in (0, 2):
+            assert np.array_equal(c.host_slot_view(c.slot(col, seg)), cols[col][seg * SEG:(seg + 1) * SEG])
+    c.begin_query()
+    done, copied = c.admit_segments([0, 2], [5, 0], [x.ctypes.data for x in cols], rows)
+    assert done == 2 and copied == 1  # segment 5 resident; segment 0's first column was copied before
