@@ -11,7 +11,10 @@ configured shapes) and larger than L2, so no flush is needed between steps.
 Beside the headline the line reports, outside the timed steps: the filter-aggregate
 (16 B/row) on the full table and on its own 6 M-row table with L2 flushed; and a batch
 of 256 generated queries run as one shared scan (CUDA graph replay) against the same
-queries run one at a time, with the results compared bit for bit.
+queries run one at a time, with the results compared bit for bit; and (at N = 1) the
+learned planner against the analytic cost model over a 600 M-row host-resident table
+with an 8 GB GPU segment cache: end-to-end ms of the same queries and the prediction
+error of each model.
 
 N > 1 runs under torchrun: rank r holds rows [r*120M, (r+1)*120M) of one table
 (weak scaling), and each step all-reduces the dense group sums over NCCL.
@@ -50,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-planner", action="store_true")
+    ap.add_argument("--planner-rows", type=int, default=600_000_000)
+    ap.add_argument("--planner-queries", type=int, default=200)
     ap.add_argument("--batch-queries", type=int, default=256)
     return ap.parse_args()
 
@@ -228,6 +234,55 @@ def batch_section(t, s, n, rank, world, args):
             "shared_scan_gbs": cols * 4 * n / batch_ms / 1e6, "shared_scan_frac_of_hbm": cols * 4 * n / batch_ms / 1e6 / peak,
             "peak_kind": peak_kind, "results_equal_one_at_a_time": equal,
             "launch": "CUDA graph replay (result memset + mask kernel + batch kernel)", "seed": SEED}
+
+
+def planner_section(args):
+    """Learned vs analytic planner over a host-resident, date-sorted fact table of
+    --planner-rows rows (1 Mi-row segments, per-segment min/max) with an 8 GB GPU segment
+    cache: the same generated queries run under each planner from the same starting
+    cache (CPU and GPU shares concurrent, results compared bit for bit); plus the mean
+    absolute error of each model's log-ms predictions on segments profiled live here."""
+    import numpy as np
+
+    from mordred_b200 import batch as B
+    from mordred_b200 import planner_experiment as PE
+    from mordred_b200.engine import SEG, Executor, SegmentedTable
+    from mordred_b200.planner import MIN_MS, AnalyticPlanner, LearnedPlanner
+
+    if not os.path.exists(PE.DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained planner weights in mordred_b200/planner_weights"}
+    learned = LearnedPlanner.load(PE.DEFAULT_WEIGHTS)
+    t0 = time.perf_counter()
+    table = SegmentedTable(args.planner_rows, SEED)
+    ex = Executor(table, cache_slots=int(8 * (1 << 30) // (SEG * 4)))
+    setup_s = time.perf_counter() - t0
+    queries = B.generate_queries(args.planner_queries, seed=SEED + 7)
+    ev = PE.evaluate(ex, [AnalyticPlanner(), learned], queries, PE.initial_weights(table, queries),
+                     log=lambda *a: None)
+    # live prediction error on freshly profiled segments (a different query seed)
+    rng = np.random.default_rng(SEED + 11)
+    feats, truth, ana = [], [], []
+    for q in B.generate_queries(40, seed=SEED + 13):
+        cand = ex.candidates(q)
+        if len(cand) == 0:
+            continue
+        recs, _ = ex.profile_segments(q, rng.choice(cand, min(16, len(cand)), replace=False))
+        for r in recs:
+            feats.append(r["features"])
+            truth.append([r["cpu_ms"], r["gpu_ms"]])
+            ana.append([r["analytic_cpu_ms"], r["analytic_gpu_ms"]])
+    truth = np.log(np.maximum(np.array(truth), MIN_MS))
+    live = {"samples": len(feats),
+            "learned": PE.mae_report(learned.predict_log(np.stack(feats)), truth),
+            "analytic": PE.mae_report(np.log(np.maximum(np.array(ana), MIN_MS)), truth)}
+    return {"fact_rows": args.planner_rows, "segments": table.nseg, "cache_slots": ex.cache.num_slots,
+            "queries": len(queries), "setup_s": setup_s,
+            "learned_ms": ev["learned"]["total_ms"], "analytic_ms": ev["analytic"]["total_ms"],
+            "speedup_learned_vs_analytic": ev["analytic"]["total_ms"] / ev["learned"]["total_ms"],
+            "per_planner": {k: ev[k] for k in ("analytic", "learned")},
+            "results_identical": ev["results_identical"], "prediction_mae_live": live,
+            "prediction_mae_training_holdout": learned.manifest.get("holdout"),
+            "weights": "mordred_b200/planner_weights/mlp.bin", "seed": SEED}
 
 
 def run_reference_arm(args, rank, world):
@@ -418,6 +473,12 @@ def main():
                "h2d_bytes_per_step": runner.h2d_bytes, "d2h_bytes_per_step": runner.d2h_bytes,
                "ms_per_step": float(ems.item()) / e_steps, "steps": e_steps}
 
+    # ---- learned vs analytic planner over a host-resident table (N = 1) --------------------
+    planner = None
+    if world == 1 and not args.no_planner:
+        torch.cuda.empty_cache()
+        planner = planner_section(args)
+
     # ---- CPU baseline on the host cores (rank 0, N = 1) -------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -463,6 +524,7 @@ def main():
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "algorithmic_bytes_per_launch": bytes_dom},
             "batched": batched,
+            "planner": planner if world == 1 else {"skipped": "the planner experiment runs at N = 1"},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": launches,

@@ -22,6 +22,7 @@ library's operators:
 """
 from __future__ import annotations
 
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -132,8 +133,8 @@ class QueryRun:
     cpu_segments: int
     waves: int
     predicted_makespan_ms: float
-    gpu_ms: float = 0.0
-    cpu_ms: float = 0.0
+    gpu_ms: float = 0.0          # device time of the GPU share (builds, copies, launches)
+    cpu_ms: float = 0.0          # wall time of the CPU share (builds, CPU engine)
     admitted: int = 0
     extra: dict = field(default_factory=dict)
 
@@ -157,6 +158,7 @@ class Executor:
         self.res_h = torch.empty(4 * ssb.QA_GROUPS, dtype=torch.int32, pin_memory=True)
         self.cpu_threads = cpu.threads()
         self._host_ptrs = [table.ptr(c, 0) if c in table.host else None for c in FACT]
+        self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
 
     # ---- planning inputs ----------------------------------------------------------------
     def candidates(self, q: B.Query) -> np.ndarray:
@@ -327,33 +329,56 @@ class Executor:
     # ---- one query -----------------------------------------------------------------------
     def run(self, q: B.Query, planner, on_gpu: np.ndarray | None = None) -> QueryRun:
         """Run q with `planner` placing its segments (or the given placement); returns the
-        merged result and timings. The GPU share is enqueued first (it only issues
-        asynchronous work), then the CPU share runs on this thread's pool while the GPU
-        works; the CPU also takes GPU segments the cache could not hold."""
+        merged result and timings. The CPU share runs on a second thread while this one
+        enqueues the GPU share (builds, admissions, launches); the CPU also takes GPU
+        segments the cache could not hold."""
         t0 = time.perf_counter()
         cand = self.candidates(q)
         self.cache.begin_query()
         span = float("nan")
+        pred = {}
         if on_gpu is None:
             pc, pg, fc, fg = planner.predict(self.context(q, cand))
             on_gpu, span = place(pc, pg, fc, fg)
+            pred = {"pred_gpu_ms": float(pg[on_gpu].sum() + (fg if on_gpu.any() else 0.0)),
+                    "pred_cpu_ms": float(pc[~on_gpu].sum() + (fc if (~on_gpu).any() else 0.0))}
+        plan_ms = (time.perf_counter() - t0) * 1e3
         gsegs = [int(s) for s in cand[on_gpu]]
         csegs = [int(s) for s in cand[~on_gpu]]
         res_len = 2 if q.template == "agg" else 4 * q.groups
         self.res_d[:res_len].zero_()
         host_res = np.zeros(res_len, np.int32)
-        waves, admitted, left = self._gpu_half(q, gsegs) if gsegs else (0, 0, [])
-        csegs += left
-        c0 = time.perf_counter()
-        if csegs:
+        # the CPU share starts at once on its own thread (the library calls release the
+        # interpreter lock), so it overlaps the GPU share's enqueueing as well as its work
+        cpu_ms = [0.0]
+
+        def cpu_share():
+            c0 = time.perf_counter()
             self._cpu_half(q, csegs, host_res)
-        cpu_ms = (time.perf_counter() - c0) * 1e3
+            cpu_ms[0] = (time.perf_counter() - c0) * 1e3
+
+        th = threading.Thread(target=cpu_share) if csegs else None
+        if th:
+            th.start()
+        self._ev[0].record()
+        waves, admitted, left = self._gpu_half(q, gsegs) if gsegs else (0, 0, [])
+        self._ev[1].record()
+        if th:
+            th.join()
+        if left:  # segments the cache could not take: the CPU runs them now
+            c0 = time.perf_counter()
+            if not csegs:
+                self.build_cpu(q)
+            self._cpu_segments(q, left, host_res)
+            cpu_ms[0] += (time.perf_counter() - c0) * 1e3
+            csegs = csegs + left
         out = self.res_h[:res_len]
         out.copy_(self.res_d[:res_len])  # waits for the GPU share
         res = merge(q, out.numpy().copy(), host_res)
         ms = (time.perf_counter() - t0) * 1e3
         return QueryRun(res, ms, len(cand), self.t.nseg - len(cand), len(gsegs) - len(left), len(csegs), waves,
-                        span, cpu_ms=cpu_ms, admitted=admitted)
+                        span, gpu_ms=self._ev[0].elapsed_time(self._ev[1]), cpu_ms=cpu_ms[0], admitted=admitted,
+                        extra=dict(pred, plan_ms=plan_ms))
 
     # ---- per-segment timing logs ------------------------------------------------------------
     def profile_segments(self, q: B.Query, segs: np.ndarray) -> tuple[list[dict], dict]:
@@ -431,8 +456,9 @@ class Executor:
 
     def _cpu_segments(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
         segs = self._order(np.array(csegs), self.t)
-        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res,
-                      segment_group=segs.astype(np.int16), segment_size=SEG)
+        group = segs.astype(np.int16)  # the arguments hold its address: keep it alive through the call
+        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res, segment_group=group,
+                      segment_size=SEG)
         cpu.star_query(a)
 
 

@@ -115,6 +115,8 @@ def evaluate(ex: Executor, planners: list, queries: list[B.Query], start_weights
         refill(ex, start_weights)
         ms, gseg, cseg, adm = [], 0, 0, 0
         res = []
+        diag = {"gpu_ms": 0.0, "cpu_ms": 0.0, "pred_gpu_ms": 0.0, "pred_cpu_ms": 0.0, "plan_ms": 0.0,
+                "cpu_bound_queries": 0}
         for q in queries:
             r = ex.run(q, p)
             ms.append(r.ms)
@@ -122,12 +124,18 @@ def evaluate(ex: Executor, planners: list, queries: list[B.Query], start_weights
             cseg += r.cpu_segments
             adm += r.admitted
             res.append(r.result)
+            diag["gpu_ms"] += r.gpu_ms
+            diag["cpu_ms"] += r.cpu_ms
+            diag["cpu_bound_queries"] += int(r.cpu_ms > r.gpu_ms)
+            for k in ("pred_gpu_ms", "pred_cpu_ms", "plan_ms"):
+                diag[k] += r.extra.get(k, 0.0)
         results[p.name] = res
         ms_sorted = sorted(ms)
         out[p.name] = {"total_ms": float(sum(ms)), "mean_ms": float(statistics.mean(ms)),
                        "p50_ms": float(ms_sorted[len(ms) // 2]),
                        "p99_ms": float(ms_sorted[min(len(ms) - 1, int(math.ceil(0.99 * len(ms))) - 1)]),
-                       "gpu_segments": gseg, "cpu_segments": cseg, "column_segments_admitted": adm}
+                       "gpu_segments": gseg, "cpu_segments": cseg, "column_segments_admitted": adm,
+                       "sums": diag}
         log(f"  {p.name}: total {out[p.name]['total_ms']:.0f} ms over {len(queries)} queries, "
             f"p50 {out[p.name]['p50_ms']:.2f}, p99 {out[p.name]['p99_ms']:.2f}, gpu/cpu segments {gseg}/{cseg}")
     names = list(results)

@@ -281,12 +281,15 @@ class HostStarRunner:
 
 
 def star_args(**kw) -> L.MbStarArgs:
-    """Build an :class:`MbStarArgs` from keyword fields (filters/probes as dict lists)."""
+    """Build an :class:`MbStarArgs` from keyword fields (filters/probes as dict lists).
+    The struct keeps a reference to every array whose address it holds, so the arrays
+    live as long as the struct does."""
     a = L.MbStarArgs()
     a.count_after = -1
     filters = kw.pop("filters", [])
     probes = kw.pop("probes", [])
     aggr = kw.pop("aggr", [])
+    a._keep = [filters, probes, aggr, dict(kw)]
     a.num_filters = len(filters)
     for i, f in enumerate(filters):
         a.filter[i] = L.MbFilter(_p(f["col"]), f.get("mode", L.MB_FILTER_BETWEEN), f["c1"], f.get("c2", 0))
