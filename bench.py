@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-planner", action="store_true")
     ap.add_argument("--planner-rows", type=int, default=600_000_000)
-    ap.add_argument("--planner-queries", type=int, default=200)
+    ap.add_argument("--planner-queries", type=int, default=300)
     ap.add_argument("--batch-queries", type=int, default=256)
     return ap.parse_args()
 
