@@ -14,7 +14,8 @@ of 256 generated queries run as one shared scan (CUDA graph replay) against the 
 queries run one at a time, with the results compared bit for bit; and (at N = 1) the
 learned planner against the analytic cost model over a 600 M-row host-resident table
 with an 8 GB GPU segment cache: end-to-end ms of the same queries and the prediction
-error of each model.
+error of each model; and (at N = 1) the serving loop: Poisson arrivals at 2,000 q/s over
+a 600 M-row GPU-resident table, p50/p99 latency, q/s and fact rows/s.
 
 N > 1 runs under torchrun: rank r holds rows [r*120M, (r+1)*120M) of one table
 (weak scaling), and each step all-reduces the dense group sums over NCCL.
@@ -57,6 +58,10 @@ def parse():
     ap.add_argument("--planner-rows", type=int, default=600_000_000)
     ap.add_argument("--planner-queries", type=int, default=300)
     ap.add_argument("--batch-queries", type=int, default=256)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rows", type=int, default=600_000_000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-seconds", type=float, default=4.0)
     return ap.parse_args()
 
 
@@ -285,6 +290,30 @@ def planner_section(args):
             "weights": "mordred_b200/planner_weights/mlp.bin", "seed": SEED}
 
 
+def serve_section(args):
+    """The serving loop: Poisson arrivals at --serve-rate over a GPU-resident table of
+    --serve-rows rows, a 16 GB admission budget, online batches of up to 256 queries
+    through the batched kernel; latency from arrival to the batch's completion."""
+    import torch
+
+    from mordred_b200 import batch as B
+    from mordred_b200 import serve as S
+    from mordred_b200 import ssb
+
+    sizes = ssb.Sizes(lo_len=args.serve_rows)
+    t = ssb.gen_device(sizes, SEED, B.BATCH_FACT, B.BATCH_DIMS)
+    srv = S.Server(t, sizes, args.serve_rows, 16 << 30)
+    n = int(args.serve_rate * args.serve_seconds)
+    qs = B.generate_queries(n, seed=SEED + 3)
+    srv.run_batch(qs[:8])
+    rep, _ = srv.serve(qs, S.poisson_arrivals(args.serve_rate, n, SEED + 5))
+    out = dict(rep.summary(args.serve_rows), rows=args.serve_rows, rate_qps=args.serve_rate, budget_bytes=16 << 30,
+               selectivity="log-uniform in [1e-5, 0.3]", seed=SEED)
+    del srv, t
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -473,6 +502,12 @@ def main():
                "h2d_bytes_per_step": runner.h2d_bytes, "d2h_bytes_per_step": runner.d2h_bytes,
                "ms_per_step": float(ems.item()) / e_steps, "steps": e_steps}
 
+    # ---- serving loop over a 600 M-row resident table (N = 1) -------------------------------
+    serving = None
+    if world == 1 and not args.no_serve:
+        torch.cuda.empty_cache()
+        serving = serve_section(args)
+
     # ---- learned vs analytic planner over a host-resident table (N = 1) --------------------
     planner = None
     if world == 1 and not args.no_planner:
@@ -525,6 +560,7 @@ def main():
                          "traffic": traffic, "algorithmic_bytes_per_launch": bytes_dom},
             "batched": batched,
             "planner": planner if world == 1 else {"skipped": "the planner experiment runs at N = 1"},
+            "serving": serving if world == 1 else {"skipped": "the serving loop runs at N = 1"},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": launches,

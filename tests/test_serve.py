@@ -1,0 +1,62 @@
+"""Serving loop: the admission controller (CPU) and the real-time server (GPU)."""
+import numpy as np
+import pytest
+
+from mordred_b200 import batch as B
+from mordred_b200 import serve as S
+
+
+def test_admission_fifo_under_budget():
+    ac = S.AdmissionController(budget_bytes=10_000, max_queue=5)
+    assert ac.arrive(0, 4096) and ac.arrive(1, 4096)
+    assert ac.arrive(2, 4096)            # does not fit yet: waits
+    assert [q for q, _ in ac.admitted] == [0, 1] and [q for q, _ in ac.waiting] == [2]
+    assert not ac.arrive(3, 20_000)      # larger than the whole budget: rejected
+    assert ac.arrive(4, 1000)            # fits, but waits behind 2: arrival order is kept
+    assert [q for q, _ in ac.waiting] == [2, 4]
+    got = ac.take(8)
+    assert [q for q, _ in got] == [0, 1] and ac.held == 8192
+    ac.release(4096)
+    assert [q for q, _ in ac.admitted] == [2, 4] and ac.held == 4096 + 4096 + 1000
+    assert ac.arrive(5, 10) and ac.arrive(6, 10) and ac.arrive(7, 10)
+    assert not ac.arrive(8, 10)          # queue limit (five queued)
+    assert ac.rejected == 2 and ac.deferred > 0
+
+
+def test_poisson_arrivals_rate():
+    a = S.poisson_arrivals(2000.0, 20_000, 1)
+    assert np.all(np.diff(a) > 0)
+    assert abs(20_000 / a[-1] - 2000.0) < 60
+
+
+def test_query_bytes_fit_in_budget():
+    qs = B.generate_queries(300, seed=2)
+    total = sum(S.query_bytes(q) for q in qs)
+    assert 0 < total < (16 << 30)
+    assert all(S.query_bytes(q) % 4096 == 0 for q in qs)
+
+
+@pytest.mark.gpu
+def test_server_answers_every_query_exactly():
+    import torch
+    from mordred_b200 import _lib as L
+    from mordred_b200 import ssb
+    torch.cuda.set_device(0)
+    n = 3_000_001
+    sizes = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(sizes, 23, B.BATCH_FACT, B.BATCH_DIMS)
+    srv = S.Server(t, sizes, n, budget_bytes=4 << 20, max_batch=64)
+    qs = B.generate_queries(300, seed=4, sel_lo=1e-4, sel_hi=0.3)
+    arr = S.poisson_arrivals(3000.0, len(qs), 6)
+    rep, res = srv.serve(qs, arr, keep_results=True)
+    s = rep.summary(n)
+    assert s["completed"] == 300 and s["rejected"] == 0 and rep.batches >= 5
+    assert max(rep.batch_sizes) <= 64 and rep.peak_held_bytes <= 4 << 20
+    assert all(x > 0 for x in rep.latencies_ms)
+    ws = B.AloneWorkspace(sizes)
+    for qid in range(0, 300, 23):
+        r = qs[qid].result_buffer()
+        B.run_alone(t, ws, qs[qid], r, n)
+        exp = r.cpu().numpy()
+        assert np.array_equal(res[qid].reshape(-1), exp.reshape(-1)), qid
+    assert L.device_status(0) == 0
