@@ -164,9 +164,10 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
   }
 }
 
-// Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes. The loads
-// of every probe are issued together; presence is then combined probe by probe in
-// order, so selection, payloads and status bits equal the sequential chain.
+// Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes. The first
+// probe's loads go out alone, then the loads of every later probe together for the rows
+// the first kept; presence is combined probe by probe in order, so selection, payloads
+// and status bits equal the sequential chain.
 template <int NSC, class L>
 __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint32_t sel, int p0, int ns,
                                             unsigned bias, Accum& A, unsigned long long* s_sum, uint32_t* s_touch,
@@ -187,48 +188,59 @@ __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint
       sv[p][i] = 0;
     }
   }
+  // two rounds: the first table probe alone, then the others together for the rows it
+  // kept (the first probe removes most rows, so later tables see a fraction of the loads,
+  // at the price of one more L2 round trip)
+  const int nsp = NSC >= 0 ? NSC : ns;
 #pragma unroll
-  for (int q = 0; q < MB_MAX_PROBES; ++q) {
-    if (q >= (NSC >= 0 ? NSC : ns)) break;
-    const int p = p0 + q;
-    ld.load(P.p_col[p], v);
-    const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
-    const int* ht = P.p_ht[p];
-    const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
+  for (int round = 0; round < 2; ++round) {
+    const int qlo = round == 0 ? 0 : 1, qhi = round == 0 ? 1 : MB_MAX_PROBES;
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      if (sel & (1u << i)) {
-        const int h = pht_slot(v[i], slots, kmin);
-        if (h < 0)
-          range_bad[q] |= 1u << i;
-        else if (bm != nullptr && !((bm[h >> 5] >> (h & 31)) & 1u))
-          absent[q] |= 1u << i;
-        else if (layout == MB_HT_KEY)
-          sv[q][i] = bm != nullptr ? 1ull : static_cast<unsigned long long>(static_cast<unsigned>(__ldg(ht + h)));
-        else
-          sv[q][i] = ldg_u64(ht + 2 * h);
+    for (int q = 0; q < MB_MAX_PROBES; ++q) {
+      if (q >= nsp) break;
+      if (q < qlo || q >= qhi) continue;
+      const int p = p0 + q;
+      ld.load(P.p_col[p], v);
+      const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
+      const int* ht = P.p_ht[p];
+      const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i) {
+        if (sel & (1u << i)) {
+          const int h = pht_slot(v[i], slots, kmin);
+          if (h < 0)
+            range_bad[q] |= 1u << i;
+          else if (bm != nullptr && !((bm[h >> 5] >> (h & 31)) & 1u))
+            absent[q] |= 1u << i;
+          else if (layout == MB_HT_KEY)
+            sv[q][i] = bm != nullptr ? 1ull : static_cast<unsigned long long>(static_cast<unsigned>(__ldg(ht + h)));
+          else
+            sv[q][i] = ldg_u64(ht + 2 * h);
+        }
       }
     }
-  }
 #pragma unroll
-  for (int q = 0; q < MB_MAX_PROBES; ++q) {
-    if (q >= (NSC >= 0 ? NSC : ns)) break;
-    const int p = p0 + q;
-    const int layout = P.p_layout[p];
+    for (int q = 0; q < MB_MAX_PROBES; ++q) {
+      if (q >= nsp) break;
+      if (q < qlo || q >= qhi) continue;
+      const int p = p0 + q;
+      const int layout = P.p_layout[p];
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      if (!(sel & (1u << i))) continue;
-      if (range_bad[q] & (1u << i)) {
-        A.bad_probe = true;
-        sel &= ~(1u << i);
-      } else if ((absent[q] & (1u << i)) || sv[q][i] == 0) {
-        sel &= ~(1u << i);
-      } else {
-        gv[q][i] = layout == MB_HT_KEY_VAL   ? static_cast<int>(sv[q][i] >> 32)
-                   : layout == MB_HT_VAL_OFF ? static_cast<int>(static_cast<unsigned>(sv[q][i]))
-                                             : 0;
+      for (int i = 0; i < ITEMS; ++i) {
+        if (!(sel & (1u << i))) continue;
+        if (range_bad[q] & (1u << i)) {
+          A.bad_probe = true;
+          sel &= ~(1u << i);
+        } else if ((absent[q] & (1u << i)) || sv[q][i] == 0) {
+          sel &= ~(1u << i);
+        } else {
+          gv[q][i] = layout == MB_HT_KEY_VAL   ? static_cast<int>(sv[q][i] >> 32)
+                     : layout == MB_HT_VAL_OFF ? static_cast<int>(static_cast<unsigned>(sv[q][i]))
+                                               : 0;
+        }
       }
     }
+    if (sel == 0) return;  // per lane; nothing warp-wide follows
   }
   if (P.count_after < 0) A.cnt += __popc(sel);
   if (sel == 0) return;
