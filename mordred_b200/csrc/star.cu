@@ -64,24 +64,38 @@ static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_b
   if (P.gmode == kGroupSmem) off += round_up(8 * P.total_val + 4 * ((P.total_val + 31) / 32), 128);
   int bm_total = 0;
   P.n_dense = 0;
+  P.sparse_p0 = 0;
   P.dense_bias = 0;
-  bool leading = true;
+  bool leading = true, payload_free = true;
   for (int p = 0; p < P.np; ++p) {
     P.p_bm_off[p] = -1;
     P.p_bm_words[p] = 0;
     const int words = (P.p_slots[p] + 31) / 32;
-    const bool have = P.p_presence[p] != nullptr || P.p_layout[p] == MB_HT_KEY;
+    // a presence bitmap comes from the caller, or the kernel derives it from the table:
+    // any MB_HT_KEY table (its test replaces the table load), and a small table with
+    // 8-byte slots when it leads the chain (its test then filters in the dense phase)
+    const bool have = P.p_presence[p] != nullptr || P.p_layout[p] == MB_HT_KEY ||
+                      (leading && P.p_slots[p] <= kBitmapDeriveMaxSlots8);
     if (stage_bitmaps && have && words * 4 <= kBitmapSmemMaxBytes && bm_total + words * 4 <= kBitmapSmemTotalBytes) {
       P.p_bm_off[p] = off;
       P.p_bm_words[p] = words;
       off += round_up(words * 4, 16);
       bm_total += words * 4;
     }
-    // a probe is answered in the dense phase when its staged bitmap alone decides it;
-    // its payload is 0, so its group term is the constant (0 - min_val) * unique_val
-    if (leading && P.p_bm_off[p] >= 0 && P.p_layout[p] == MB_HT_KEY) {
+    // leading probes with a staged bitmap are tested in the dense phase. One whose
+    // payload nobody reads (an MB_HT_KEY table, or a zero group multiplier with the
+    // payload not stored) is settled there: its group term is the constant
+    // (0 - min_val) * unique_val. The others are probed again in the sparse phase, for
+    // the survivors only, to read their payloads.
+    if (leading && P.p_bm_off[p] >= 0) {
       P.n_dense = p + 1;
-      P.dense_bias += (0u - static_cast<unsigned>(P.p_min[p])) * static_cast<unsigned>(P.p_mul[p]);
+      const bool free = P.p_layout[p] == MB_HT_KEY || (P.p_mul[p] == 0 && P.p_res_slot[p] < 0);
+      if (payload_free && free) {
+        P.sparse_p0 = p + 1;
+        P.dense_bias += (0u - static_cast<unsigned>(P.p_min[p])) * static_cast<unsigned>(P.p_mul[p]);
+      } else {
+        payload_free = false;
+      }
     } else {
       leading = false;
     }
@@ -210,7 +224,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   if (smem > budget) smem = layout_smem(P, ncw, items, 2, false);
   if (smem > budget) return MB_ERR_SIZE;
 
-  const Variant* var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.n_dense);
+  const Variant* var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0);
   if (var == nullptr) return MB_ERR_ARG;
 
   int grid = a->grid;

@@ -28,6 +28,7 @@ constexpr int kMaxStages = 8;
 constexpr int kSmemGroupMax = 8192;            // groups kept in shared memory per CTA
 constexpr int kBitmapSmemMaxBytes = 32768;     // largest presence bitmap staged (262,144 slots)
 constexpr int kBitmapSmemTotalBytes = 40960;
+constexpr int kBitmapDeriveMaxSlots8 = 65536;  // largest 8-byte-slot table whose bitmap a CTA derives
 
 enum GroupMode { kGroupScalar = 0, kGroupSmem = 1, kGroupGlobal = 2 };
 
@@ -39,8 +40,11 @@ struct StarPlan {
   int nf;
   int f_col[MB_MAX_FILTERS], f_mode[MB_MAX_FILTERS], f_c1[MB_MAX_FILTERS], f_c2[MB_MAX_FILTERS];
   int np;
-  int n_dense;                    // leading probes answered by a staged bitmap alone
-  unsigned dense_bias;            // their group terms (0 - min_val) * unique_val, summed
+  int n_dense;                    // leading probes tested against a staged presence bitmap
+  int sparse_p0;                  // first probe of the sparse phase: the leading bitmap-tested
+                                  // probes whose payload is not needed stop before it, the
+                                  // others are probed again there for their payload
+  unsigned dense_bias;            // group terms (0 - min_val) * unique_val of probes < sparse_p0
   int p_col[MB_MAX_PROBES];
   const int* p_ht[MB_MAX_PROBES];
   int p_slots[MB_MAX_PROBES], p_kmin[MB_MAX_PROBES], p_layout[MB_MAX_PROBES];

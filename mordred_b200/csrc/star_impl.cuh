@@ -377,6 +377,31 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     const int words = P.p_bm_words[p];
     if (P.p_presence[p] != nullptr) {
       for (int w = tid; w < words; w += NWARPS * 32) bm[w] = __ldg(P.p_presence[p] + w);
+    } else if (P.p_layout[p] != MB_HT_KEY) {
+      // derive presence from a table with 8-byte slots: slot s is present when nonzero
+      const int slots = P.p_slots[p];
+      const unsigned long long* ht = reinterpret_cast<const unsigned long long*>(P.p_ht[p]);
+      const bool vec = aligned16_dev(ht);
+      for (int w = tid; w < words; w += NWARPS * 32) {
+        uint32_t word = 0;
+        if (vec && (w + 1) * 32 <= slots) {
+          // four 16-byte loads (8 slots) in flight at a time: few registers, so the set-up
+          // does not raise the kernel's register count
+          const ulonglong2* src = reinterpret_cast<const ulonglong2*>(ht + w * 32);
+#pragma unroll 1
+          for (int j0 = 0; j0 < 16; j0 += 4) {
+            ulonglong2 q[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) q[j] = __ldg(src + j0 + j);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              word |= ((q[j].x != 0ull ? 1u : 0u) << (2 * (j0 + j))) | ((q[j].y != 0ull ? 1u : 0u) << (2 * (j0 + j) + 1));
+          }
+        } else {
+          for (int j = 0; j < 32 && w * 32 + j < slots; ++j) word |= (__ldg(ht + w * 32 + j) != 0ull ? 1u : 0u) << j;
+        }
+        bm[w] = word;
+      }
     } else {
       // derive presence from an MB_HT_KEY table: each thread folds 32 slots into a word
       // with its eight 16-byte loads in flight together
@@ -457,8 +482,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     // ---- consumers ---------------------------------------------------------------------
     const int cw = warp - 1;
     uint16_t* list = reinterpret_cast<uint16_t*>(smem + P.smem_list_off) + cw * WROWS;
-    const int nd = NDC >= 0 ? NDC : P.n_dense;
-    const int ns = NSC >= 0 ? NSC : P.np - P.n_dense;
+    const int nd = P.sparse_p0;  // the sparse phase starts at probe sparse_p0 <= n_dense
+    const int ns = NSC >= 0 ? NSC : P.np - P.sparse_p0;
     const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
     int s = 0;
     uint32_t phase = 0;

@@ -13,8 +13,8 @@ static const Variant kSpecial[] = {
     MB_SHAPE_VARIANTS(3, 0, 0),  // filter-aggregate (q11.cu)
     MB_SHAPE_VARIANTS(0, 1, 2),  // Query A: supplier bitmap, part and date tables (q21.cu)
     MB_SHAPE_VARIANTS(0, 1, 3),  // Query B: supplier bitmap, customer, part, date (q41.cu)
-    MB_SHAPE_VARIANTS(2, 0, 4),  // engine filter_probe_group_by over four tables
-    MB_SHAPE_VARIANTS(0, 0, 4),  // engine probe_group_by over four tables
+    MB_SHAPE_VARIANTS(2, 1, 4),  // engine filter_probe_group_by: supplier bitmap, four tables
+    MB_SHAPE_VARIANTS(0, 1, 4),  // engine probe_group_by: supplier bitmap, four tables
     MB_SHAPE_VARIANTS(0, 0, 1),  // src/ops probe, one table
 };
 
