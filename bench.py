@@ -357,7 +357,7 @@ def main():
     import torch.distributed as dist
 
     from mordred_b200 import _lib as L
-    from mordred_b200 import ssb
+    from mordred_b200 import shard, ssb
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -368,24 +368,14 @@ def main():
     s = ssb.Sizes(lo_len=n)
     dims = sorted(set(ssb.QA_DIMS + ssb.QB_DIMS))
     # rank r holds rows [r*n, (r+1)*n) of one fact table; dimensions are replicated
-    t = {}
-    st = ssb._stream()
-    for name in ssb.QB_FACT + ["lo_discount", "lo_quantity", "lo_extendedprice"]:
-        buf = torch.empty(n, dtype=torch.int32, device="cuda")
-        L.call("mb_gen_fact_column", ssb.FACT_COLUMNS[name], SEED, rank * n, n, s.s_len, s.c_len, s.p_len,
-               ssb._p(buf), st)
-        t[name] = buf
+    t = shard.gen_shard(s, SEED, ssb.QB_FACT + ["lo_discount", "lo_quantity", "lo_extendedprice"], rank, n)
     t.update(ssb.gen_device(s, SEED, [], dims))
     ws = ssb.StarWorkspace(s)
     dense = torch.zeros(ssb.QA_GROUPS + ssb.QB_GROUPS, dtype=torch.int64, device="cuda")
 
     def combine():
         # the only exchange: dense group sums of both queries, summed over ranks
-        ra = ws["res_a"].view(-1, 4)[:, 2:4].contiguous().view(torch.int64).view(-1)
-        rb = ws["res_b"].view(-1, 4)[:, 2:4].contiguous().view(torch.int64).view(-1)
-        dense[: ssb.QA_GROUPS].copy_(ra)
-        dense[ssb.QA_GROUPS:].copy_(rb)
-        dist.all_reduce(dense)
+        shard.allreduce_sums([shard.crystal4_sums(ws["res_a"]), shard.crystal4_sums(ws["res_b"])], dense)
 
     # per-step events around each probe launch, on the stream the kernels run on
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
