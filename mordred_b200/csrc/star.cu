@@ -89,7 +89,9 @@ static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_b
     // the survivors only, to read their payloads.
     if (leading && P.p_bm_off[p] >= 0) {
       P.n_dense = p + 1;
-      const bool free = P.p_layout[p] == MB_HT_KEY || (P.p_mul[p] == 0 && P.p_res_slot[p] < 0);
+      // (MB_AGG_MUL_PAYLOAD multiplies by the first probe's payload: that one is never free)
+      const bool free = (P.p_layout[p] == MB_HT_KEY || (P.p_mul[p] == 0 && P.p_res_slot[p] < 0)) &&
+                        !(p == 0 && P.agg_op == MB_AGG_MUL_PAYLOAD);
       if (payload_free && free) {
         P.sparse_p0 = p + 1;
         P.dense_bias += (0u - static_cast<unsigned>(P.p_min[p])) * static_cast<unsigned>(P.p_mul[p]);

@@ -185,8 +185,11 @@ def test_pht_builds_bit_identical():
     assert status() == 0
 
 
-def test_src_ops_join():
-    n_dim, n_fact = 100_000, 3_000_011
+@pytest.mark.parametrize("n_dim", [50_000, 100_000])
+def test_src_ops_join(n_dim):
+    """src/ops join at two table sizes: 100,000 slots are probed in L2; 50,000 get a
+    presence bitmap that the dense phase tests, and the payload is read afterwards."""
+    n_fact = 3_000_011
     g = torch.Generator(device="cpu").manual_seed(1)
     dim_key = torch.randperm(n_dim, generator=g).to(torch.int32) + 1
     dim_val = torch.randint(-5000, 5000, (n_dim,), generator=g, dtype=torch.int32)
