@@ -453,7 +453,7 @@ def main():
         for _ in range(reps + 2):
             if do_flush:
                 flush.zero_()
-                torch.sum(clean, dtype=torch.int64, out=sink)
+                sink.add_(clean.sum(dtype=torch.int64))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             ssb.q11(t, rows, ws, zero=False)
