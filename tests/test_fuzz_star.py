@@ -7,8 +7,9 @@ offsets, fills from empty to full and some keys below key_min (a probe-range sta
 group multipliers and minima that can push rows outside [0, total_val) (a group-range
 status), every aggregate and every result layout, a selection count after a random
 filter, caller-supplied presence bitmaps, and a random launch shape. The CUDA kernel
-(`mb_star_query`, gpu) and the library's CPU operator (`mb_cpu_star_query`) must both
-reproduce the oracle's result array and status bits.
+(`mb_star_query`, gpu; direct columns and segment-cache addressing) and the library's
+CPU operator (`mb_cpu_star_query`) must both reproduce the oracle's result array and
+status bits.
 """
 import numpy as np
 import pytest
@@ -19,9 +20,10 @@ from mordred_b200 import cpu, ssb
 from oracle import oracle as O
 
 
-def make_case(seed: int) -> dict:
+def make_case(seed: int, n: int | None = None) -> dict:
     rng = np.random.default_rng(seed)
-    n = int(rng.choice([0, 1, 33, 2048, 4099, 65_537, 250_001, 1_000_003]))
+    drawn = int(rng.choice([0, 1, 33, 2048, 4099, 65_537, 250_001, 1_000_003]))
+    n = drawn if n is None else n
 
     def fact_col(lo, hi):
         return rng.integers(lo, hi, n, dtype=np.int64).astype(np.int32)
@@ -117,17 +119,17 @@ def result_array(case):
     return np.zeros((6 if rl == L.MB_RES_ENGINE6 else 4) * tv, np.int32)
 
 
-def oracle_run(case):
+def oracle_run(case, rows=None, **segments):
     res = result_array(case)
     cnt = np.zeros(1, np.uint64)
-    st = O.star(case["n"], filters=case["filters"], probes=case["probes"], aggr=case["aggr"], agg_op=case["agg_op"],
-                total_val=case["total_val"], group_bias=case["group_bias"], res_layout=case["res_layout"], res=res,
-                count=cnt if case["count_after"] is not None else None,
-                count_after=case["count_after"] if case["count_after"] is not None else -1)
+    st = O.star(case["n"] if rows is None else rows, filters=case["filters"], probes=case["probes"],
+                aggr=case["aggr"], agg_op=case["agg_op"], total_val=case["total_val"], group_bias=case["group_bias"],
+                res_layout=case["res_layout"], res=res, count=cnt if case["count_after"] is not None else None,
+                count_after=case["count_after"] if case["count_after"] is not None else -1, **segments)
     return res, int(cnt[0]), st
 
 
-def args_for(case, conv, res, cnt, launch):
+def args_for(case, conv, res, cnt, launch, rows=None):
     """MbStarArgs with every array passed through `conv` (host numpy or device tensor)."""
     filters = [dict(f, col=conv(f["col"])) for f in case["filters"]]
     probes = []
@@ -139,8 +141,8 @@ def args_for(case, conv, res, cnt, launch):
     kw = dict(launch)
     if case["count_after"] is not None:
         kw.update(count=cnt, count_after=case["count_after"])
-    return ssb.star_args(num_rows=case["n"], filters=filters, probes=probes, aggr=[conv(a) for a in case["aggr"]],
-                         agg_op=case["agg_op"], total_val=case["total_val"], group_bias=case["group_bias"],
+    return ssb.star_args(num_rows=case["n"] if rows is None else rows, filters=filters, probes=probes,
+                         aggr=[conv(a) for a in case["aggr"]], agg_op=case["agg_op"], total_val=case["total_val"], group_bias=case["group_bias"],
                          res_layout=case["res_layout"], res=res, **kw)
 
 
@@ -179,6 +181,74 @@ def test_cuda_kernel_matches_oracle(seed):
             ssb.star_query(args_for(case, dev, res, cnt, launch))
         except L.MbError as e:
             # a drawn launch shape whose stages cannot fit next to this case's columns
+            assert e.code == L.MB_ERR_SIZE and launch, e
+            continue
+        torch.cuda.synchronize()
+        assert L.device_status(0, clear=True) == est, launch
+        assert np.array_equal(comparable(case, res.cpu().numpy()), comparable(case, exp)), launch
+        if case["count_after"] is not None:
+            assert int(cnt.cpu().numpy()[0]) == ecnt, launch
+
+
+def _fact_arrays(case):
+    cols = [f["col"] for f in case["filters"]] + [q["fkey"] for q in case["probes"]] + list(case["aggr"])
+    return list({id(a): a for a in cols}.values())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(60))
+def test_cuda_kernel_segment_cache_matches_oracle(seed):
+    """The same random queries over a segment cache: every fact column's segments sit at
+    shuffled slots of one cache array (the engine's gpuCache), columns are per-segment
+    slot indices, and the call's rows are either a list of segments (a permutation of a
+    subset, the last one cut short) or a run from a segment-aligned start offset."""
+    rng = np.random.default_rng(9000 + seed)
+    seg = int(rng.choice([1 << 14, 1 << 16]))
+    nphys = int(rng.integers(1, 7))
+    case = make_case(9000 + seed, n=nphys * seg)
+    if rng.random() < 0.5:
+        k = int(rng.integers(1, nphys + 1))
+        seg_list = rng.permutation(nphys)[:k].astype(np.int16)
+        start, rows = 0, k * seg - int(rng.integers(0, seg))
+    else:
+        seg_list = None
+        j = int(rng.integers(0, nphys))
+        start, rows = j * seg, int(rng.integers(0, (nphys - j) * seg + 1))
+    exp, ecnt, est = oracle_run(case, rows, segment_group=seg_list, start_offset=start, segment_size=seg)
+
+    torch.cuda.set_device(0)
+    L.call("mb_init", 0)
+    L.device_status(0, clear=True)
+    keep = []
+
+    def dev(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        keep.append(t)
+        return t
+
+    facts = _fact_arrays(case)
+    nslots = len(facts) * nphys + 2
+    perm = rng.permutation(nslots)
+    cache = np.zeros(nslots * seg, np.int32)
+    col_idx = {}
+    for ci, arr in enumerate(facts):
+        slots = perm[ci * nphys:(ci + 1) * nphys]
+        for sg in range(nphys):
+            cache[slots[sg] * seg:(slots[sg] + 1) * seg] = arr[sg * seg:(sg + 1) * seg]
+        col_idx[id(arr)] = dev(slots.astype(np.int32))
+    cache_dev = dev(cache)
+    seg_dev = dev(seg_list) if seg_list is not None else None
+
+    def conv(a):
+        return col_idx[id(a)] if id(a) in col_idx else dev(a)
+
+    for launch in (case["launch"], {}):
+        res = dev(result_array(case))
+        cnt = dev(np.zeros(1, np.uint64))
+        kw = dict(launch, gpu_cache=cache_dev, segment_group=seg_dev, start_offset=start, segment_size=seg)
+        try:
+            ssb.star_query(args_for(case, conv, res, cnt, kw, rows=rows))
+        except L.MbError as e:
             assert e.code == L.MB_ERR_SIZE and launch, e
             continue
         torch.cuda.synchronize()
