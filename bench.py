@@ -314,9 +314,22 @@ def serve_section(args):
     return out
 
 
+def workload_config(n, s, world):
+    """The `config` object both arms print: the workload named by what it is."""
+    return {"workload": f"star join + group-by: Query A (category=1, region=1, group year x brand "
+                        f"7x1000) + Query B (c_region=1, s_region=1, mfgr in {{0,1}}, group year x "
+                        f"c_nation 7x25) over {n:,} fact rows per GPU",
+            "fact_rows_per_gpu": n, "dims": {"supplier": s.s_len, "customer": s.c_len,
+                                             "part": s.p_len, "date": s.d_len},
+            "l2": f"{n * 16 / 1e9:.2f} GB + {n * 24 / 1e9:.2f} GB of fact columns per step"
+                  + (", larger than the 126 MB L2, no flush" if n * 16 > 126e6 else ", within L2"),
+            "parallelism": f"row shards x{world}", "seed": SEED}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
+    from mordred_b200 import ssb
     from oracle import oracle as O
 
     rows = min(args.rows, args.cpu_sample_rows * 5)
@@ -334,8 +347,8 @@ def run_reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32 (int64 sums)", "data": "synthetic",
-        "config": {"workload": f"Query A + Query B over {rows:,} fact rows on the host CPU "
-                               "(src/cpu/ssb/q21.cpp + q41.cpp)", "fact_rows": rows},
+        "config": dict(workload_config(rows, ssb.Sizes(lo_len=rows), 1),
+                       executed_on="host CPU: the reference's own engine, src/cpu/ssb/q21.cpp + q41.cpp"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{rows:,} fact rows per query, {args.steps} timed trials"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -533,13 +546,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32 (int64 sums)", "data": "synthetic",
-            "config": {"workload": f"star join + group-by: Query A (category=1, region=1, group year x brand "
-                                   f"7x1000) + Query B (c_region=1, s_region=1, mfgr in {{0,1}}, group year x "
-                                   f"c_nation 7x25) over {n:,} fact rows per GPU",
-                       "fact_rows_per_gpu": n, "dims": {"supplier": s.s_len, "customer": s.c_len,
-                                                        "part": s.p_len, "date": s.d_len},
-                       "l2": "inputs larger than L2 (1.92 GB + 2.88 GB per step), no flush",
-                       "parallelism": f"row shards x{world}", "seed": SEED},
+            "config": workload_config(n, s, world),
             "per_query": {
                 "filter_aggregate": {"ms": f_full, "fact_rows_per_s": n / (f_full / 1e3),
                                      "gbs": n * 16 / f_full / 1e6, "frac_of_hbm": n * 16 / f_full / 1e6 / peak},
