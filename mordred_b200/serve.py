@@ -15,10 +15,14 @@ src/gpudb/main.cu:72-489, one at a time). Here:
   Poisson times; whenever the GPU is idle the server takes every admitted waiting query
   (up to the batch limit), plans the batch, runs it and reads the results back. A
   query's latency is its batch's completion time minus its arrival time.
+* :class:`CircularServer` — the table is cut into chunks that batched launches visit in
+  a cycle; admitted queries join at the next launch and finish after one lap, so a
+  query waits about one scan instead of the batch in progress plus its own.
 """
 from __future__ import annotations
 
 import collections
+import ctypes as C
 import math
 import statistics
 import time
@@ -97,6 +101,7 @@ class ServeReport:
     rejected: int = 0
     deferred: int = 0
     peak_held_bytes: int = 0
+    scan_rows: int = 0          # fact rows the launches scanned
 
     def summary(self, rows: int) -> dict:
         lat = sorted(self.latencies_ms)
@@ -106,7 +111,7 @@ class ServeReport:
                 "p50_ms": pct(0.50), "p90_ms": pct(0.90), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None,
                 "batches": self.batches, "mean_batch": statistics.mean(self.batch_sizes) if self.batch_sizes else 0,
                 "mean_batch_ms": statistics.mean(self.batch_ms) if self.batch_ms else 0,
-                "fact_rows_per_s": self.batches * rows / self.seconds if self.seconds else None,
+                "fact_rows_per_s": (self.scan_rows or self.batches * rows) / self.seconds if self.seconds else None,
                 "query_rows_per_s": len(lat) * rows / self.seconds if self.seconds else None,
                 "rejected": self.rejected, "deferred_admissions": self.deferred,
                 "peak_admitted_bytes": self.peak_held_bytes}
@@ -174,6 +179,125 @@ class Server:
         return rep, results
 
 
+@dataclass
+class _Member:
+    qid: int
+    nbytes: int
+    query: B.Query
+    cq: L.MbBatchQuery          # the query's launch descriptor, made once at admission
+    res: torch.Tensor           # its device result, accumulated over the chunks
+    launched: int = 0           # chunks launched for it so far
+    last_event: object = None   # completion event of its last chunk
+
+
+class CircularServer:
+    """Cooperative circular scan: the GPU-resident table is split into `chunks` row
+    ranges that one batched launch after another visits in a cycle. An admitted query
+    joins the running scan at the next launch and completes once every chunk has been
+    launched for it (one full lap from wherever it joined), so it waits for about one
+    scan of the table rather than for the batch in progress plus its own. Every query
+    sees every row exactly once and the kernel only adds into its result, so results are
+    those of the query run alone. Up to 256 queries share a launch; a second launch is
+    queued before the first completes so the GPU never waits for the host."""
+
+    def __init__(self, t: dict, sizes: ssb.Sizes, n_rows: int, budget_bytes: int = 16 << 30,
+                 max_active: int = L.MB_BATCH_MAX_QUERIES, chunks: int = 8):
+        self.t, self.sizes, self.n = t, sizes, n_rows
+        self.pats = B.build_pats(t, sizes)
+        self.dims = self.pats.c_dims()
+        self.budget = budget_bytes
+        self.max_active = max_active
+        step = -(-n_rows // max(1, chunks))
+        step = -(-step // 4096) * 4096  # 16-byte aligned chunk starts
+        self.bounds = [(r0, min(n_rows, r0 + step)) for r0 in range(0, n_rows, step)] or [(0, 0)]
+        self.ws = torch.empty(16, dtype=torch.uint8, device=next(iter(t.values())).device)
+
+    def _launch(self, c: int, members: list) -> None:
+        r0, r1 = self.bounds[c]
+        arr = (L.MbBatchQuery * len(members))(*[m.cq for m in members])
+        a = L.MbBatchArgs()
+        a.num_rows = r1 - r0
+        for i, name in enumerate(B.BATCH_FACT):
+            col = self.t[name]
+            a.fact[i] = col.data_ptr() + r0 * col.element_size()
+        a.dim = self.dims
+        a.num_queries = len(members)
+        a.queries = C.cast(arr, C.POINTER(L.MbBatchQuery))
+        a.smem_group_bytes = -1
+        need = int(L.lib().mb_batch_workspace_bytes(C.byref(a)))
+        if need > self.ws.numel():
+            torch.cuda.current_stream().synchronize()  # launches in flight use the old workspace
+            self.ws = torch.empty(max(need, 2 * self.ws.numel()), dtype=torch.uint8, device=self.ws.device)
+        a.workspace, a.workspace_bytes = self.ws.data_ptr(), self.ws.numel()
+        L.check("mb_batch_run", L.lib().mb_batch_run(C.byref(a), ssb._stream()))
+
+    def serve(self, queries: list[B.Query], arrivals: np.ndarray, max_wait_s: float = 60.0,
+              keep_results: bool = False) -> tuple[ServeReport, dict]:
+        """Serve `queries` arriving at `arrivals` (s, ascending) in real time."""
+        ac = AdmissionController(self.budget)
+        rep = ServeReport(len(queries), 0.0)
+        results = {}
+        nbytes = [query_bytes(q) for q in queries]
+        nchunks = len(self.bounds)
+        active: list[_Member] = []            # still have chunks to be launched
+        inflight: collections.deque = collections.deque()  # (event, members finishing with it, launch time)
+        c = 0
+        done = 0
+        i = 0
+        t0 = time.perf_counter()
+        while done + ac.rejected < len(queries):
+            now = time.perf_counter() - t0
+            while i < len(queries) and arrivals[i] <= now:
+                ac.arrive(i, nbytes[i])
+                i += 1
+            for qid, nb in ac.take(self.max_active - len(active)):
+                res = queries[qid].result_buffer()
+                active.append(_Member(qid, nb, queries[qid], queries[qid].to_c(res), res))
+            rep.peak_held_bytes = max(rep.peak_held_bytes, ac.held)
+            if active and len(inflight) < 2:
+                members = list(active)
+                self._launch(c, members)
+                ev = torch.cuda.Event()
+                ev.record()
+                finishing = []
+                for m in members:
+                    m.launched += 1
+                    if m.launched == nchunks:
+                        finishing.append(m)
+                active = [m for m in active if m.launched < nchunks]
+                inflight.append((ev, finishing, time.perf_counter()))
+                rep.batches += 1
+                rep.batch_sizes.append(len(members))
+                rep.scan_rows += self.bounds[c][1] - self.bounds[c][0]
+                c = (c + 1) % nchunks
+                continue
+            if inflight:
+                ev, finishing, tl = inflight.popleft()
+                ev.synchronize()
+                end = time.perf_counter() - t0
+                rep.batch_ms.append((time.perf_counter() - tl) * 1e3)
+                if finishing:
+                    host = torch.cat([m.res.reshape(-1).view(torch.uint8) for m in finishing]).cpu()
+                    off = 0
+                    for m in finishing:
+                        nb = m.res.numel() * m.res.element_size()
+                        if keep_results:
+                            results[m.qid] = host[off: off + nb].numpy().view(
+                                np.int64 if m.query.template == "agg" else np.int32).copy()
+                        off += nb
+                        rep.latencies_ms.append((end - arrivals[m.qid]) * 1e3)
+                        ac.release(m.nbytes)
+                    done += len(finishing)
+                continue
+            if i < len(queries):
+                time.sleep(max(0.0, min(arrivals[i] - now, 0.001)))
+            elif now > max_wait_s:
+                break
+        rep.seconds = time.perf_counter() - t0
+        rep.rejected, rep.deferred = ac.rejected, ac.deferred
+        return rep, results
+
+
 def main():
     import argparse
     import json
@@ -184,17 +308,20 @@ def main():
     ap.add_argument("--seconds", type=float, default=5.0)
     ap.add_argument("--seed", type=int, default=20260101)
     ap.add_argument("--budget-gb", type=float, default=16.0)
+    ap.add_argument("--chunks", type=int, default=0, help="circular scan over this many chunks (0: whole-scan batches)")
     args = ap.parse_args()
     torch.cuda.set_device(0)
     L.call("mb_init", 0)
     sizes = ssb.Sizes(lo_len=args.rows)
     t = ssb.gen_device(sizes, args.seed, B.BATCH_FACT, B.BATCH_DIMS)
-    srv = Server(t, sizes, args.rows, int(args.budget_gb * (1 << 30)))
+    budget = int(args.budget_gb * (1 << 30))
+    srv = CircularServer(t, sizes, args.rows, budget, chunks=args.chunks) if args.chunks else \
+        Server(t, sizes, args.rows, budget)
     n = int(args.rate * args.seconds)
     qs = B.generate_queries(n, seed=args.seed + 3)
-    srv.run_batch(qs[:8])  # load the kernels
+    (srv if isinstance(srv, Server) else Server(t, sizes, args.rows, budget)).run_batch(qs[:8])  # load kernels
     rep, _ = srv.serve(qs, poisson_arrivals(args.rate, n, args.seed + 5))
-    print(json.dumps(dict(rep.summary(args.rows), rows=args.rows, rate_qps=args.rate,
+    print(json.dumps(dict(rep.summary(args.rows), rows=args.rows, rate_qps=args.rate, chunks=args.chunks,
                           budget_bytes=srv.budget, device_status=L.device_status(0))), flush=True)
 
 

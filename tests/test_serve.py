@@ -60,3 +60,32 @@ def test_server_answers_every_query_exactly():
         exp = r.cpu().numpy()
         assert np.array_equal(res[qid].reshape(-1), exp.reshape(-1)), qid
     assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("chunks", [1, 5])
+def test_circular_server_answers_every_query_exactly(chunks):
+    """Queries that join a circular scan between chunks get exactly the results of
+    running alone, whatever chunk they joined at."""
+    import torch
+    from mordred_b200 import _lib as L
+    from mordred_b200 import ssb
+    torch.cuda.set_device(0)
+    n = 3_000_001
+    sizes = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(sizes, 29, B.BATCH_FACT, B.BATCH_DIMS)
+    srv = S.CircularServer(t, sizes, n, budget_bytes=4 << 20, max_active=64, chunks=chunks)
+    assert len(srv.bounds) == chunks and srv.bounds[-1][1] == n
+    qs = B.generate_queries(300, seed=5, sel_lo=1e-4, sel_hi=0.3)
+    arr = S.poisson_arrivals(3000.0, len(qs), 7)
+    rep, res = srv.serve(qs, arr, keep_results=True)
+    s = rep.summary(n)
+    assert s["completed"] == 300 and s["rejected"] == 0
+    assert max(rep.batch_sizes) <= 64 and rep.peak_held_bytes <= 4 << 20
+    assert all(x > 0 for x in rep.latencies_ms)
+    ws = B.AloneWorkspace(sizes)
+    for qid in range(0, 300, 7):
+        r = qs[qid].result_buffer()
+        B.run_alone(t, ws, qs[qid], r, n)
+        assert np.array_equal(res[qid].reshape(-1), r.cpu().numpy().reshape(-1)), qid
+    assert L.device_status(0) == 0
