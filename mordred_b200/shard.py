@@ -2,7 +2,7 @@
 of one table (the seeded generator takes a row offset, so every shard is a slice of the
 same table) and replicated dimension tables; the only exchange is one all-reduce of the
 queries' dense group sums (64-bit integer sums are exact in any order). The reference
-has no multi-GPU path; this is the row partitioning SURVEY-style star queries allow.
+has no multi-GPU path; star queries over independent fact rows partition this way.
 """
 from __future__ import annotations
 
