@@ -50,8 +50,17 @@ struct __align__(16) AQ {
   unsigned kmul0, kmul1, bias;
   int total;                // groups (1 for a scalar)
   int soff;                 // shared-memory byte offset of the 64-bit sums, -1: atomics in L2
-  int flags;                // bits 0-1 agg op, bit 2 CRYSTAL4 keys, bits 3-4 number of keys
+  int flags;                // bits 0-1 agg op, bit 2 CRYSTAL4 keys, bits 3-4 number of keys,
+                            // bits 8-16 queries in its family, bits 17-25 its place in it
 };
+// A family is a set of queries with the same group count whose shared-memory sums are
+// interleaved group-major: the sum of group g of the family's j-th query lies at
+// base + 8 * (g * members + j) (soff = base + 8 * j), so the matches of one row — same
+// group, neighbouring queries — hit neighbouring words rather than banks at random. The
+// members' touch bitmaps follow the sums: base + 8 * total * members + 4 * words * j.
+// A query alone is a family of one (the plain layout).
+__device__ __forceinline__ int aq_family(const AQ& A) { return (A.flags >> 8) & 0x1ff; }
+__device__ __forceinline__ int aq_member(const AQ& A) { return (A.flags >> 17) & 0x1ff; }
 static_assert(sizeof(AQ) == 32, "aggregation descriptor size");
 
 // Per-query descriptor in the launch parameters (96 bytes).
@@ -159,10 +168,12 @@ __device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int
   }
   const bool c4 = (A.flags >> 2) & 1;
   if (A.soff >= 0) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff) + g, w);
+    const int fam = aq_family(A), j = aq_member(A);
+    atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff) + g * fam, w);
     if (!c4) return;
     // the first row of a group in this CTA writes the group's keys
-    uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + A.soff + 8 * A.total);
+    uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + A.soff - 8 * j + 8 * A.total * fam) +
+                        j * ((A.total + 31) >> 5);
     const uint32_t bit = 1u << (g & 31);
     if ((s_touch[g >> 5] & bit) || (atomicOr(&s_touch[g >> 5], bit) & bit)) return;
   } else {
@@ -494,8 +505,9 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
     if (A.soff < 0) continue;
     const unsigned long long* s_sum = reinterpret_cast<const unsigned long long*>(smem + A.soff);
     const bool c4 = (A.flags >> 2) & 1;
+    const int fam = aq_family(A);
     for (int g = tid; g < A.total; g += NWARPS * 32) {
-      const unsigned long long v = s_sum[g];
+      const unsigned long long v = s_sum[g * fam];
       if (v == 0) continue;
       atomicAdd(c4 ? reinterpret_cast<unsigned long long*>(static_cast<int*>(s_res[q]) + 4 * g + 2)
                    : static_cast<unsigned long long*>(s_res[q]) + g,
@@ -652,7 +664,7 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
                    (nk > 1 ? static_cast<unsigned>(q.key_min[1]) * A.kmul1 : 0u));
     A.total = q.res_layout == MB_RES_SCALAR ? 1 : q.total_val;
     A.soff = -1;
-    A.flags = q.agg_op | ((q.res_layout == MB_RES_CRYSTAL4 ? 1 : 0) << 2) | (nk << 3);
+    A.flags = q.agg_op | ((q.res_layout == MB_RES_CRYSTAL4 ? 1 : 0) << 2) | (nk << 3) | (1 << 8);
     d.res = q.res;
   }
   // constrained attributes and the hull of the ranges on each
@@ -899,16 +911,42 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   P.smem_groups_off = off;
   int groups_bytes = 0;
   const int group_cap = a->smem_group_bytes < 0 ? 131072 : a->smem_group_bytes;
-  for (int pass_total = 1; pass_total <= 1024; pass_total *= 2) {
+  // queries with the same group count form a family (group-major interleaved sums); as
+  // many members as fit, smallest group counts first
+  for (;;) {
+    int total = 0;
+    for (int qi = 0; qi < P.nq; ++qi) {
+      const AQ& A = P.q[qi].a;
+      if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total > 1024 || (A.flags & (1 << 30))) continue;
+      if (total == 0 || A.total < total) total = A.total;
+    }
+    if (total == 0) break;
+    const int words = (total + 31) / 32;
+    auto fam_bytes = [&](int k) { return (8 * total * k + 4 * words * k + 15) / 16 * 16; };
+    int members = 0;
+    for (int qi = 0; qi < P.nq; ++qi) {
+      const AQ& A = P.q[qi].a;
+      if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total != total) continue;
+      if (groups_bytes + fam_bytes(members + 1) > group_cap ||
+          total_smem(off + groups_bytes + fam_bytes(members + 1), stages) > budget)
+        break;
+      ++members;
+    }
+    int j = 0;
     for (int qi = 0; qi < P.nq; ++qi) {
       AQ& A = P.q[qi].a;
-      if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total > pass_total) continue;
-      const int bytes = (8 * A.total + 4 * ((A.total + 31) / 32) + 15) / 16 * 16;
-      if (groups_bytes + bytes > group_cap || total_smem(off + groups_bytes + bytes, stages) > budget) continue;
-      A.soff = off + groups_bytes;
-      groups_bytes += bytes;
+      if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total != total) continue;
+      if (j < members) {
+        A.soff = off + groups_bytes + 8 * j;
+        A.flags = (A.flags & 0xff) | (members << 8) | (j << 17);
+        ++j;
+      } else {
+        A.flags |= 1 << 30;  // no room: sums by L2 atomics (marked so the search moves on)
+      }
     }
+    groups_bytes += fam_bytes(members);
   }
+  for (int qi = 0; qi < P.nq; ++qi) P.q[qi].a.flags &= ~(1 << 30);
   P.smem_groups_words = groups_bytes / 4;
   P.smem_stage_off = (off + groups_bytes + 127) / 128 * 128;
   const int smem = total_smem(off + groups_bytes, stages);
