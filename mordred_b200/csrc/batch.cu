@@ -185,8 +185,10 @@ __device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int
   }
   int* res = static_cast<int*>(s_res[qi]);
   const int nk = (A.flags >> 3) & 3;
-  if (nk > 0) res[4 * g] = k0;
-  if (nk > 1) res[4 * g + 1] = k1;
+  if (nk > 1)
+    *reinterpret_cast<int2*>(res + 4 * g) = make_int2(k0, k1);  // one 8-byte store (16-byte records)
+  else if (nk > 0)
+    res[4 * g] = k0;
 }
 
 // The queries accepting one row: presence mask AND one mask per constrained attribute.
