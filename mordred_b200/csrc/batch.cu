@@ -49,7 +49,8 @@ struct __align__(16) AQ {
   uint16_t a0, a1, k0, k1;  // stage field codes
   unsigned kmul0, kmul1, bias;
   int total;                // groups (1 for a scalar)
-  int soff;                 // shared-memory byte offset of the 64-bit sums, -1: atomics in L2
+  int soff;                 // shared-memory byte offset of the 64-bit sums; < 0: sums by L2
+                            // atomics, and soff <= -2 puts the keys' touch bitmap at -soff - 2
   int flags;                // bits 0-1 agg op, bit 2 CRYSTAL4 keys, bits 3-4 number of keys,
                             // bits 8-16 queries in its family, bits 17-25 its place in it
 };
@@ -182,6 +183,12 @@ __device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int
                  : static_cast<unsigned long long*>(res) + g,
               w);
     if (!c4) return;
+    if (A.soff <= -2) {
+      // keys once per CTA and group: the group records are few lines that every SM updates
+      uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + (-A.soff - 2));
+      const uint32_t bit = 1u << (g & 31);
+      if ((s_touch[g >> 5] & bit) || (atomicOr(&s_touch[g >> 5], bit) & bit)) return;
+    }
   }
   int* res = static_cast<int*>(s_res[qi]);
   const int nk = (A.flags >> 3) & 3;
@@ -949,6 +956,20 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
     groups_bytes += fam_bytes(members);
   }
   for (int qi = 0; qi < P.nq; ++qi) P.q[qi].a.flags &= ~(1 << 30);
+  // queries left with L2 sums that write keys, and few groups (a few hot result lines),
+  // get a touch bitmap in shared memory where it fits (smallest group counts first), so
+  // they write their keys once per CTA and group; with many groups the stores spread out
+  // and cost less than the test
+  for (int pass_total = 1; pass_total <= 1024; pass_total *= 2) {
+    for (int qi = 0; qi < P.nq; ++qi) {
+      AQ& A = P.q[qi].a;
+      if (A.soff != -1 || !((A.flags >> 2) & 1) || A.total > pass_total || A.total <= pass_total / 2) continue;
+      const int bytes = (4 * ((A.total + 31) / 32) + 15) / 16 * 16;
+      if (total_smem(off + groups_bytes + bytes, stages) > budget) continue;
+      A.soff = -(off + groups_bytes) - 2;
+      groups_bytes += bytes;
+    }
+  }
   P.smem_groups_words = groups_bytes / 4;
   P.smem_stage_off = (off + groups_bytes + 127) / 128 * 128;
   const int smem = total_smem(off + groups_bytes, stages);
