@@ -920,6 +920,15 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   P.smem_groups_off = off;
   int groups_bytes = 0;
   const int group_cap = a->smem_group_bytes < 0 ? 131072 : a->smem_group_bytes;
+  // shared memory kept for the touch bitmaps of the small-array queries that end up with
+  // L2 sums (below): a few bytes each, and without one such a query writes its keys on
+  // every match
+  int touch_reserve = 0;
+  for (int qi = 0; qi < P.nq; ++qi) {
+    const AQ& A = P.q[qi].a;
+    if (P.q[qi].res_layout != MB_RES_SCALAR && ((A.flags >> 2) & 1) && A.total <= 1024)
+      touch_reserve += (4 * ((A.total + 31) / 32) + 15) / 16 * 16;
+  }
   // queries with the same group count form a family (group-major interleaved sums); as
   // many members as fit, smallest group counts first
   for (;;) {
@@ -937,7 +946,7 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
       const AQ& A = P.q[qi].a;
       if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total != total) continue;
       if (groups_bytes + fam_bytes(members + 1) > group_cap ||
-          total_smem(off + groups_bytes + fam_bytes(members + 1), stages) > budget)
+          total_smem(off + groups_bytes + fam_bytes(members + 1) + touch_reserve, stages) > budget)
         break;
       ++members;
     }
