@@ -187,7 +187,6 @@ class _Member:
     cq: L.MbBatchQuery          # the query's launch descriptor, made once at admission
     res: torch.Tensor           # its device result, accumulated over the chunks
     launched: int = 0           # chunks launched for it so far
-    last_event: object = None   # completion event of its last chunk
 
 
 class CircularServer:
