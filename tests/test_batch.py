@@ -52,6 +52,31 @@ def test_batch_equals_alone(n_rows, n_queries):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("template,group_bytes", [("qb", -1), ("qb", 0), ("qb", 16384), ("qa", -1), ("mixed", 65536)])
+def test_batch_group_placements_equal_alone(template, group_bytes):
+    """256 queries of one form (or mixed) under shared-memory budgets that put group
+    sums in shared-memory families, in L2 with per-CTA key touch bitmaps, or in L2 with
+    keys written on every match: every result equals the query run alone."""
+    import torch
+    from mordred_b200 import _lib as L
+    torch.cuda.set_device(0)
+    n_rows = 2_000_003
+    s = ssb.Sizes(lo_len=n_rows, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(s, 77, B.BATCH_FACT, B.BATCH_DIMS)
+    pats = B.build_pats(t, s)
+    kw = {} if template == "mixed" else {"templates": (template,)}
+    qs = B.generate_queries(256, seed=5, sel_lo=1e-3, sel_hi=0.3, **kw)
+    res_b = [q.result_buffer() for q in qs]
+    B.run_batch(t, pats, qs, res_b, n_rows, smem_group_bytes=group_bytes)
+    ws = B.AloneWorkspace(s)
+    for i, q in enumerate(qs):
+        r = q.result_buffer()
+        B.run_alone(t, ws, q, r, n_rows)
+        assert np.array_equal(res_b[i].cpu().numpy(), r.cpu().numpy()), (i, q.template)
+    assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
 def test_batch_launch_configs_and_oracle():
     import torch
     from mordred_b200 import _lib as L
