@@ -61,6 +61,14 @@ typedef void* mb_stream_t;
 #define MB_HT_KEY 0
 #define MB_HT_KEY_VAL 1
 #define MB_HT_VAL_OFF 2
+/* No table: the probe passes through the group value an earlier join found. fkey is an
+ * int list of dimension rows read at the call's row position k (an offset list's dim_off
+ * array, or indexed by row when the call has no list), ht is the dimension column (or its
+ * per-segment cache-slot array under segment addressing) read at that dimension row, and
+ * num_slots the dimension's rows (a row outside [0, num_slots) sets
+ * MB_STATUS_PROBE_RANGE and is dropped). Every row is present.
+ * (BlockReadFilteredOffset, src/gpudb/BlockLibrary.cuh:484-541; GPUProcessing.h:198-205) */
+#define MB_HT_PASS 3
 
 /* Aggregates (int32 arithmetic, then widened to 64 bits, as q11.cu:74, q41.cu:76). */
 #define MB_AGG_SUM 0   /* a0           */
@@ -123,6 +131,13 @@ typedef struct mb_star_args {
   int stages;                 /* 2..8 bulk-copy stages */
   int grid;                   /* CTAs; 0 = one wave of resident CTAs */
   int group_mode;             /* 0 auto, 1 groups in shared memory (flushed per CTA), 2 global atomics per row */
+  /* Offset-list input (optional): rows[k], k < num_rows, is the physical fact row the call
+   * visits at position k (an offset list from mb_star_select, or from the CPU). Columns are
+   * read at rows[k] (under segment addressing through the slot of segment rows[k] >>
+   * log2(segment_size); segment_group and start_offset are then unused). The GPU3 forms of
+   * the engine kernels (src/gpudb/GPUProcessing.h:157-273, 393-494, 1385-1524, 1610-1846).
+   * The launch fields above are ignored for a list. */
+  const int* rows;
 } mb_star_args;
 
 /* Fused filter -> chained probe -> group-by/aggregate over the fact table.
@@ -250,6 +265,67 @@ int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs,
                   const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table,
                   int start_offset, const short* segment_group, mb_stream_t stream);
 
+/* KernelArgs.h:306-315 offsetGPU (declared here for the offset-list forms below): a list of
+ * physical fact rows and, per dimension slot 1..4 (supplier, customer, part, date), the
+ * dimension row each fact row joined with. */
+typedef struct mb_offsetGPU {
+  int* lo_off;
+  int* dim_off1; int* dim_off2; int* dim_off3; int* dim_off4;
+} mb_offsetGPU;
+
+/* ---- offset-list (GPU3) forms and the remaining engine kernels --------------------
+ * The list forms visit the num_tuples physical fact rows of offset->lo_off. For a
+ * dimension slot with both key_idx and ht set the row probes that (VAL_OFF) table; for a
+ * slot with only gargs->group_idx set the group value is gpuCache's dimension column
+ * group_idx read at the row's offset->dim_off entry (an earlier join's match, which the
+ * caller guarantees is a row of that dimension); other slots contribute group value 0.
+ * Group-by forms: res = int[6*total_val], sum of aggr1 - aggr2 (gargs->mode 1: aggr1 *
+ * aggr2); aggregate forms: u64 sum of aggr1 * aggr2 at res[4]. */
+/* GPUProcessing.h:157-273 filter_probe_group_by_GPU3 (filters BETWEEN compare1..2, 3..4). */
+int mb_filter_probe_group_by_GPU3(const int* gpuCache, const mb_offsetGPU* offset,
+                                  const mb_filterArgsGPU* fargs, const mb_probeArgsGPU* pargs,
+                                  const mb_groupbyArgsGPU* gargs, int num_tuples, int* res,
+                                  mb_stream_t stream);
+/* GPUProcessing.h:393-494 probe_group_by_GPU3. */
+int mb_probe_group_by_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_probeArgsGPU* pargs,
+                           const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, mb_stream_t stream);
+/* GPUProcessing.h:1385-1470 groupByGPU: no probes; every listed row is grouped by the
+ * passed-through group values. */
+int mb_groupByGPU(const int* gpuCache, const mb_offsetGPU* offset, const mb_groupbyArgsGPU* gargs,
+                  int num_tuples, int* res, mb_stream_t stream);
+/* GPUProcessing.h:1472-1524 aggregationGPU: u64 sum of aggr1 * aggr2 over lo_off at res[4]
+ * (a missing aggregate column reads as 0, as BlockSetValue, so nothing is added). */
+int mb_aggregationGPU(const int* gpuCache, const int* lo_off, const mb_groupbyArgsGPU* gargs,
+                      int num_tuples, int* res, mb_stream_t stream);
+/* GPUProcessing.h:1526-1608 probe_aggr_GPU2: the date probe (slot 4) only, then the
+ * aggregate, over a segment range. */
+int mb_probe_aggr_GPU2(const int* gpuCache, const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs,
+                       int num_tuples, int* res, int start_offset, const short* segment_group,
+                       mb_stream_t stream);
+/* GPUProcessing.h:1610-1673 probe_aggr_GPU3: probe_aggr_GPU2 over an offset list. */
+int mb_probe_aggr_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_probeArgsGPU* pargs,
+                       const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, mb_stream_t stream);
+/* GPUProcessing.h:1778-1846 filter_probe_aggr_GPU3: the second filter (compare3..4) only —
+ * the first ran where the list was made — then the date probe and the aggregate. */
+int mb_filter_probe_aggr_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_filterArgsGPU* fargs,
+                              const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs, int num_tuples,
+                              int* res, mb_stream_t stream);
+/* GPUProcessing.h:999-1028 build_GPU3: the engine build over the dimension rows listed in
+ * dim_off (row id = the listed row); no filter (fargs->filter_idx1 must be NULL). */
+int mb_build_GPU3(const int* gpuCache, const int* dim_off, const mb_filterArgsGPU* fargs,
+                  const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table, mb_stream_t stream);
+/* GPUProcessing.h:1030-1113 build_GPU_minmax: build_GPU2 that also folds the smallest and
+ * largest key of the rows passing the filter into *min_global / *max_global (device ints,
+ * initialised by the caller; each CTA starts from bargs->val_max / val_min as the
+ * reference's blocks do). */
+int mb_build_GPU_minmax(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_buildArgsGPU* bargs,
+                        int num_tuples, int* hash_table, int* min_global, int* max_global, int start_offset,
+                        const short* segment_group, mb_stream_t stream);
+/* GPUProcessing.h:1115-1172 build_GPU_minmax2: build_GPU3 with the key range. */
+int mb_build_GPU_minmax2(const int* gpuCache, const int* dim_off, const mb_filterArgsGPU* fargs,
+                         const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table, int* min_global,
+                         int* max_global, mb_stream_t stream);
+
 /* ---- batched multi-query execution ------------------------------------------------ */
 /* Many star queries over one resident fact table in one launch: every fact tile is
  * loaded once, each dimension is read once per row through a packed attribute table
@@ -331,12 +407,6 @@ size_t mb_batch_workspace_bytes(const mb_batch_args* args);
 int mb_batch_run(const mb_batch_args* args, mb_stream_t stream);
 
 /* ---- selection with compaction: offset lists for CPU/GPU handoff ---------------- */
-/* KernelArgs.h:306-315 offsetGPU: a list of physical fact rows and, per dimension slot
- * 1..4 (supplier, customer, part, date), the dimension offset each row joined with. */
-typedef struct mb_offsetGPU {
-  int* lo_off;
-  int* dim_off1; int* dim_off2; int* dim_off3; int* dim_off4;
-} mb_offsetGPU;
 
 /* Rows passing args' filters and probes (aggregation fields ignored) appended to an
  * offset list: lo_off[k] = physical row (start_offset + row, or the segment-mapped row
@@ -453,6 +523,18 @@ int mb_cpu_build_pht(const int* filter_col, int filter_mode, int c1, int c2,
 int mb_cpu_star_query(const mb_star_args* args, const int* rows, int64_t num_listed,
                       int nthreads, unsigned int* status);
 
+/* Selection with compaction on the host (filter_CPU / filter_probe_CPU / probe_CPU and their
+ * list forms, src/gpudb/CPUProcessing.cu:3-437,1158-1333): the rows of the call (its
+ * virtual rows, mapped through segment_group as in mb_cpu_star_query, or the listed ones)
+ * passing a's filters and probes, written in row order: lo_off[k] = physical row,
+ * dim_off[p][k] (optional per probe) = ht[2h+1] - 1 for VAL_OFF tables (the dimension
+ * row), the payload for KEY_VAL, 0 for KEY. *total = rows passing; entries past capacity
+ * are counted, not written, and set MB_STATUS_OVERFLOW in *status. The CPU half of a
+ * query split CPU-select -> GPU-aggregate (the GPU3 forms above take the list). */
+int mb_cpu_star_select(const mb_star_args* a, const int* rows, int64_t num_listed, int* lo_off,
+                       int* const* dim_off, int64_t capacity, int64_t* total, int nthreads,
+                       unsigned int* status);
+
 /* ---- GPU segment cache (src/gpudb/CacheManager.{h,cu}) ---------------------------- */
 /* Fact columns are split into segments of segment_size rows (reference SEGMENT_SIZE,
  * common.h:73). The cache owns one device pool of num_slots segment slots — the
@@ -532,6 +614,10 @@ int mb_device_status(int device, unsigned int* status, int clear);
 const char* mb_error_string(int code);
 /* Number of kernel launches issued by this library in this process (all devices). */
 unsigned long long mb_launch_count(void);
+/* 1 when the library's per-device state (the status word it cudaMalloc's and the kernel
+ * attributes mb_init sets) exists on `device`, else 0. Touches no device and allocates
+ * nothing: a caller can check that only allocation-free entry points ran. */
+int mb_device_state_ready(int device);
 
 #ifdef __cplusplus
 }

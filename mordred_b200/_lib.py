@@ -21,7 +21,7 @@ MB_STATUS_TIMEOUT = 0x4
 MB_STATUS_OVERFLOW = 0x8
 
 MB_FILTER_EQ, MB_FILTER_BETWEEN, MB_FILTER_EQ_OR_EQ = 0, 1, 2
-MB_HT_KEY, MB_HT_KEY_VAL, MB_HT_VAL_OFF = 0, 1, 2
+MB_HT_KEY, MB_HT_KEY_VAL, MB_HT_VAL_OFF, MB_HT_PASS = 0, 1, 2, 3
 MB_AGG_SUM, MB_AGG_SUB, MB_AGG_MUL, MB_AGG_MUL_PAYLOAD = 0, 1, 2, 3
 MB_RES_SCALAR, MB_RES_ENGINE6, MB_RES_CRYSTAL4, MB_RES_DENSE = 0, 1, 2, 3
 MB_MAX_FILTERS, MB_MAX_PROBES = 3, 4
@@ -55,7 +55,7 @@ class MbStarArgs(C.Structure):
                 ("segment_group", C.c_void_p), ("start_offset", C.c_int64),
                 ("segment_size", C.c_int), ("threads", C.c_int),
                 ("items_per_thread", C.c_int), ("stages", C.c_int), ("grid", C.c_int),
-                ("group_mode", C.c_int)]
+                ("group_mode", C.c_int), ("rows", C.c_void_p)]
 
 
 class MbFilterArgsGPU(C.Structure):
@@ -115,6 +115,7 @@ SIGNATURES = {
     "mb_device_status": (I, [I, PS(C.c_uint), I]),
     "mb_error_string": (C.c_char_p, [I]),
     "mb_launch_count": (C.c_ulonglong, []),
+    "mb_device_state_ready": (I, [I]),
 }
 
 
@@ -241,6 +242,18 @@ SIGNATURES.update({
     "mb_filter_probe_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbFilterArgsGPU), PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P,
                                  P]),
     "mb_probe_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbProbeArgsGPU), PS(MbOffsetGPU), I, P, P]),
+    "mb_filter_probe_group_by_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbFilterArgsGPU), PS(MbProbeArgsGPU),
+                                          PS(MbGroupbyArgsGPU), I, P, P]),
+    "mb_probe_group_by_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbProbeArgsGPU), PS(MbGroupbyArgsGPU), I, P, P]),
+    "mb_groupByGPU": (I, [P, PS(MbOffsetGPU), PS(MbGroupbyArgsGPU), I, P, P]),
+    "mb_aggregationGPU": (I, [P, P, PS(MbGroupbyArgsGPU), I, P, P]),
+    "mb_probe_aggr_GPU2": (I, [P, PS(MbProbeArgsGPU), PS(MbGroupbyArgsGPU), I, P, I, P, P]),
+    "mb_probe_aggr_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbProbeArgsGPU), PS(MbGroupbyArgsGPU), I, P, P]),
+    "mb_filter_probe_aggr_GPU3": (I, [P, PS(MbOffsetGPU), PS(MbFilterArgsGPU), PS(MbProbeArgsGPU),
+                                      PS(MbGroupbyArgsGPU), I, P, P]),
+    "mb_build_GPU3": (I, [P, P, PS(MbFilterArgsGPU), PS(MbBuildArgsGPU), I, P, P]),
+    "mb_build_GPU_minmax": (I, [P, PS(MbFilterArgsGPU), PS(MbBuildArgsGPU), I, P, P, P, I, P, P]),
+    "mb_build_GPU_minmax2": (I, [P, P, PS(MbFilterArgsGPU), PS(MbBuildArgsGPU), I, P, P, P, P]),
     "mb_segcache_create": (P, [I, I64, I, I, I, I]),
     "mb_segcache_destroy": (None, [P]),
     "mb_segcache_pool": (P, [P]),
@@ -257,6 +270,7 @@ SIGNATURES.update({
     "mb_cpu_threads": (I, []),
     "mb_cpu_build_pht": (I, [P, I, I, I, P, P, I, P, I, I, I, I, PS(C.c_uint)]),
     "mb_cpu_star_query": (I, [PS(MbStarArgs), P, I64, I, PS(C.c_uint)]),
+    "mb_cpu_star_select": (I, [PS(MbStarArgs), P, I64, P, P, I64, PS(C.c_int64), I, PS(C.c_uint)]),
     "mb_pat_build": (I, [P, I, I, I, P, I, P, I, P, I, P, P]),
     "mb_batch_workspace_bytes": (C.c_size_t, [PS(MbBatchArgs)]),
     "mb_batch_run": (I, [PS(MbBatchArgs), P]),

@@ -33,3 +33,23 @@ def star_query(args: L.MbStarArgs, rows: np.ndarray | None = None, nthreads: int
         rows = np.ascontiguousarray(rows, dtype=np.int32)
     L.call("mb_cpu_star_query", C.byref(args), _p(rows), 0 if rows is None else len(rows), nthreads, C.byref(st))
     return st.value
+
+
+def star_select(args: L.MbStarArgs, rows: np.ndarray | None = None, capacity: int | None = None,
+                nthreads: int = 0):
+    """Rows passing the pipeline's filters and probes over host columns, in row order:
+    (lo_off, [dim_off per probe], status bits) — the CPU side of a CPU-select ->
+    GPU-aggregate split (the offset list the GPU3 forms take)."""
+    st = C.c_uint(0)
+    if rows is not None:
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+    n = len(rows) if rows is not None else int(args.num_rows)
+    cap = n if capacity is None else capacity
+    lo = np.empty(max(cap, 1), np.int32)
+    dims = [np.empty(max(cap, 1), np.int32) for _ in range(args.num_probes)]
+    arr = (C.c_void_p * 4)(*[d.ctypes.data for d in dims], *([None] * (4 - len(dims))))
+    total = C.c_int64(0)
+    L.call("mb_cpu_star_select", C.byref(args), _p(rows), 0 if rows is None else len(rows), lo.ctypes.data,
+           C.cast(arr, C.c_void_p), cap, C.byref(total), nthreads, C.byref(st))
+    k = min(int(total.value), cap)
+    return lo[:k], [d[:k] for d in dims], st.value

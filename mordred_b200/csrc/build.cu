@@ -32,9 +32,23 @@ struct BuildPlan {
   long long start_offset;
   int seg_shift;
   unsigned int* status;
+  const int* rows;     // optional list of dimension rows to build from (build_GPU3 forms)
+  int* min_out;        // optional key range of the rows passing the filter (minmax forms)
+  int* max_out;
+  int val_min, val_max;  // where each warp's range starts (the reference's block start values)
 };
 
 __device__ __forceinline__ long long build_row_index(const BuildPlan& B, long long r, int* seg_out) {
+  if (B.rows != nullptr) {
+    // a listed dimension row: the physical row, through its own segment's slot
+    const long long d = __ldg(B.rows + r);
+    if (B.gpu_cache == nullptr) {
+      *seg_out = 0;
+      return d;
+    }
+    *seg_out = static_cast<int>(d >> B.seg_shift);
+    return d & ((1ll << B.seg_shift) - 1);
+  }
   if (B.gpu_cache == nullptr) {
     *seg_out = 0;
     return r;
@@ -52,12 +66,15 @@ __device__ __forceinline__ int build_load(const BuildPlan& B, const int* col, in
 
 __global__ void build_kernel(const __grid_constant__ BuildPlan B) {
   bool bad = false;
+  int kmin = B.val_max, kmax = B.val_min;
   for (long long r = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; r < B.n;
        r += static_cast<long long>(gridDim.x) * blockDim.x) {
     int seg;
     const long long idx = build_row_index(B, r, &seg);
     if (B.filter != nullptr && !build_pass(build_load(B, B.filter, seg, idx), B.mode, B.c1, B.c2)) continue;
     const int key = build_load(B, B.key, seg, idx);
+    kmin = key < kmin ? key : kmin;
+    kmax = key > kmax ? key : kmax;
     const int d = key - B.kmin;
     const int h = (d >= 0 && d < B.slots) ? d : d % B.slots;
     if (h < 0) {
@@ -75,9 +92,11 @@ __global__ void build_kernel(const __grid_constant__ BuildPlan B) {
       present = key != 0 || v != 0;
     } else {
       // engine layout: the row id is the dimension row's position in the table
-      // (segment * segment_size + in-segment offset), stored +1 so 0 stays "empty".
-      const long long rowid = B.gpu_cache == nullptr ? B.start_offset + r
-                                                     : (static_cast<long long>(seg) << B.seg_shift) + idx;
+      // (segment * segment_size + in-segment offset, or the listed row), stored +1 so 0
+      // stays "empty".
+      const long long rowid = B.rows != nullptr       ? static_cast<long long>(__ldg(B.rows + r))
+                              : B.gpu_cache == nullptr ? B.start_offset + r
+                                                       : (static_cast<long long>(seg) << B.seg_shift) + idx;
       if (B.val != nullptr) atomicCAS(B.ht + 2ll * h, 0, build_load(B, B.val, seg, idx));
       B.ht[2ll * h + 1] = static_cast<int>(rowid + 1);
       present = true;
@@ -85,6 +104,16 @@ __global__ void build_kernel(const __grid_constant__ BuildPlan B) {
     if (B.presence != nullptr && present) atomicOr(B.presence + (h >> 5), 1u << (h & 31));
   }
   if (bad) set_status(B.status, MB_STATUS_PROBE_RANGE);
+  if (B.min_out != nullptr) {
+    // every warp folds its range in, starting from (val_max, val_min) as the reference's
+    // blocks do (GPUProcessing.h:1052,1101-1110)
+    kmin = __reduce_min_sync(0xffffffffu, kmin);
+    kmax = __reduce_max_sync(0xffffffffu, kmax);
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(B.min_out, kmin);
+      atomicMax(B.max_out, kmax);
+    }
+  }
 }
 
 static int launch_build(BuildPlan& B, cudaStream_t stream) {
@@ -136,15 +165,26 @@ extern "C" int mb_join_build(const int* dim_key, const int* dim_val, int num_tup
   return mb_build_pht(nullptr, 0, 0, 0, dim_key, dim_val, num_tuples, hash_table, num_slots, 0, nullptr, stream);
 }
 
-extern "C" int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_buildArgsGPU* bargs,
-                             int num_tuples, int* hash_table, int start_offset, const short* segment_group,
-                             mb_stream_t stream) {
+// The engine builds (VAL_OFF layout): build_GPU2 / build_GPU_minmax over a segment range,
+// build_GPU3 / build_GPU_minmax2 over a list of dimension rows (dim_off), the minmax forms
+// also folding the key range into *min_out / *max_out.
+static int engine_build(const int* gpuCache, const int* dim_off, const mb_filterArgsGPU* fargs,
+                        const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table, int start_offset,
+                        const short* segment_group, int* min_out, int* max_out, mb_stream_t stream) {
   if (num_tuples == 0) return MB_OK;
   if (bargs == nullptr || bargs->key_idx == nullptr || hash_table == nullptr || num_tuples < 0 ||
       bargs->num_slots <= 0)
     return MB_ERR_ARG;
+  if ((min_out == nullptr) != (max_out == nullptr)) return MB_ERR_ARG;
   if (!aligned8(hash_table)) return MB_ERR_ALIGN;
+  // the list forms take no filter (GPUProcessing.h:1018, cudaAssert(fargs.filter_idx1 == NULL))
+  if (dim_off != nullptr && fargs != nullptr && fargs->filter_idx1 != nullptr) return MB_ERR_ARG;
   BuildPlan B = {};
+  B.rows = dim_off;
+  B.min_out = min_out;
+  B.max_out = max_out;
+  B.val_min = bargs->val_min;
+  B.val_max = bargs->val_max;
   if (fargs != nullptr && fargs->filter_idx1 != nullptr) {
     if (fargs->mode1 < MB_FILTER_EQ || fargs->mode1 > MB_FILTER_EQ_OR_EQ) return MB_ERR_ARG;
     B.filter = fargs->filter_idx1;
@@ -160,8 +200,37 @@ extern "C" int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs,
   B.kmin = bargs->val_min;
   B.layout = MB_HT_VAL_OFF;
   B.gpu_cache = gpuCache;
-  B.seg_group = segment_group;
-  B.start_offset = start_offset;
+  B.seg_group = dim_off != nullptr ? nullptr : segment_group;
+  B.start_offset = dim_off != nullptr ? 0 : start_offset;
   B.seg_shift = 20;  // SEGMENT_SIZE = 1,048,576 (src/gpudb/common.h:73)
   return launch_build(B, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int mb_build_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_buildArgsGPU* bargs,
+                             int num_tuples, int* hash_table, int start_offset, const short* segment_group,
+                             mb_stream_t stream) {
+  return engine_build(gpuCache, nullptr, fargs, bargs, num_tuples, hash_table, start_offset, segment_group, nullptr,
+                      nullptr, stream);
+}
+
+extern "C" int mb_build_GPU3(const int* gpuCache, const int* dim_off, const mb_filterArgsGPU* fargs,
+                             const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table, mb_stream_t stream) {
+  if (dim_off == nullptr) return MB_ERR_ARG;
+  return engine_build(gpuCache, dim_off, fargs, bargs, num_tuples, hash_table, 0, nullptr, nullptr, nullptr, stream);
+}
+
+extern "C" int mb_build_GPU_minmax(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_buildArgsGPU* bargs,
+                                   int num_tuples, int* hash_table, int* min_global, int* max_global,
+                                   int start_offset, const short* segment_group, mb_stream_t stream) {
+  if (min_global == nullptr || max_global == nullptr) return MB_ERR_ARG;
+  return engine_build(gpuCache, nullptr, fargs, bargs, num_tuples, hash_table, start_offset, segment_group,
+                      min_global, max_global, stream);
+}
+
+extern "C" int mb_build_GPU_minmax2(const int* gpuCache, const int* dim_off, const mb_filterArgsGPU* fargs,
+                                    const mb_buildArgsGPU* bargs, int num_tuples, int* hash_table, int* min_global,
+                                    int* max_global, mb_stream_t stream) {
+  if (dim_off == nullptr || min_global == nullptr || max_global == nullptr) return MB_ERR_ARG;
+  return engine_build(gpuCache, dim_off, fargs, bargs, num_tuples, hash_table, 0, nullptr, min_global, max_global,
+                      stream);
 }

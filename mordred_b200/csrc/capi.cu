@@ -34,6 +34,7 @@ static int init_device_locked(int dev) {
   ds.status = status;
   int e = star_init_device(ds);
   if (e == MB_OK) e = batch_init_device(ds);
+  if (e == MB_OK) e = list_init_device(ds);
   if (e != MB_OK) return e;
   ds.device = dev;
   return MB_OK;
@@ -138,6 +139,12 @@ const char* mb_error_string(int code) {
 
 unsigned long long mb_launch_count(void) { return g_launches.load(); }
 
+int mb_device_state_ready(int device) {
+  if (device < 0 || device >= 64) return 0;
+  std::lock_guard<std::mutex> lk(g_state_mu);
+  return g_state[device].device == device ? 1 : 0;
+}
+
 int mb_star_query(const mb_star_args* args, mb_stream_t stream) {
   return launch_star(args, static_cast<cudaStream_t>(stream), 0);
 }
@@ -231,31 +238,52 @@ int mb_join_probe(const int* fact_fkey, const int* fact_val, int num_tuples, con
 }
 
 // ---- engine wrappers ---------------------------------------------------------------------
-static int engine_star(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_probeArgsGPU* pargs,
-                       const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, int start_offset,
-                       const short* segment_group, mb_stream_t stream, bool group_by, bool probe_only_date) {
-  if (pargs == nullptr || gargs == nullptr || res == nullptr || num_tuples < 0) return MB_ERR_ARG;
+// Engine kernels restated on the fused pipeline. `off` (list forms) names the physical fact
+// rows to visit and the dimension offsets earlier joins produced; slots whose group value
+// comes from such an offset read gargs' dimension column there (MB_HT_PASS).
+enum EngineFilters { kEngineBothFilters, kEngineSecondFilter };
+
+static int engine_star(const int* gpuCache, const mb_offsetGPU* off, const mb_filterArgsGPU* fargs,
+                       const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs, int num_tuples, int* res,
+                       int start_offset, const short* segment_group, mb_stream_t stream, bool group_by,
+                       bool probe_only_date, EngineFilters filters = kEngineBothFilters) {
+  if (gargs == nullptr || res == nullptr || num_tuples < 0) return MB_ERR_ARG;
+  if (off != nullptr && off->lo_off == nullptr) return MB_ERR_ARG;
   if (num_tuples == 0) return MB_OK;
   mb_star_args a;
   memset(&a, 0, sizeof(a));
   a.num_rows = num_tuples;
+  a.rows = off != nullptr ? off->lo_off : nullptr;
   if (fargs != nullptr) {
-    // fact-side filters are BETWEEN compare1..compare2 / compare3..compare4 (GPUProcessing.h:74-86)
-    if (fargs->filter_idx1) a.filter[a.num_filters++] = {fargs->filter_idx1, MB_FILTER_BETWEEN, fargs->compare1, fargs->compare2};
+    // fact-side filters are BETWEEN compare1..compare2 / compare3..compare4 (GPUProcessing.h:74-86);
+    // filter_probe_aggr_GPU3 applies the second only (GPUProcessing.h:1808-1812)
+    if (fargs->filter_idx1 && filters == kEngineBothFilters)
+      a.filter[a.num_filters++] = {fargs->filter_idx1, MB_FILTER_BETWEEN, fargs->compare1, fargs->compare2};
     if (fargs->filter_idx2) a.filter[a.num_filters++] = {fargs->filter_idx2, MB_FILTER_BETWEEN, fargs->compare3, fargs->compare4};
   }
+  static const mb_probeArgsGPU kNoProbes = {};
+  if (pargs == nullptr) pargs = &kNoProbes;
   const int* keys[4] = {pargs->key_idx1, pargs->key_idx2, pargs->key_idx3, pargs->key_idx4};
   const int* hts[4] = {pargs->ht1, pargs->ht2, pargs->ht3, pargs->ht4};
   const int lens[4] = {pargs->dim_len1, pargs->dim_len2, pargs->dim_len3, pargs->dim_len4};
   const int kmins[4] = {pargs->min_key1, pargs->min_key2, pargs->min_key3, pargs->min_key4};
   const int mins[4] = {gargs->min_val1, gargs->min_val2, gargs->min_val3, gargs->min_val4};
   const int uniq[4] = {gargs->unique_val1, gargs->unique_val2, gargs->unique_val3, gargs->unique_val4};
+  const int* groups[4] = {gargs->group_idx1, gargs->group_idx2, gargs->group_idx3, gargs->group_idx4};
+  const int* doffs[4] = {off ? off->dim_off1 : nullptr, off ? off->dim_off2 : nullptr, off ? off->dim_off3 : nullptr,
+                         off ? off->dim_off4 : nullptr};
   int bias = 0;
   for (int s = 0; s < 4; ++s) {
-    if (probe_only_date && s != 3) continue;  // filter_probe_aggr_GPU2 probes slot 4 only (GPUProcessing.h:1737)
+    if (probe_only_date && s != 3) continue;  // the aggregate kernels probe slot 4 only (GPUProcessing.h:1737)
     if (keys[s] != nullptr && hts[s] != nullptr) {
       a.probe[a.num_probes++] = {keys[s], hts[s], lens[s], kmins[s], MB_HT_VAL_OFF,
                                  mins[s], group_by ? uniq[s] : 0, group_by ? s : -1, nullptr};
+    } else if (group_by && off != nullptr && groups[s] != nullptr) {
+      // the value an earlier join found: the dimension column at the listed dimension row
+      // (GPUProcessing.h:198-205); the reference does not bound the row, so neither is it
+      // bounded here beyond being non-negative
+      if (doffs[s] == nullptr) return MB_ERR_ARG;
+      a.probe[a.num_probes++] = {doffs[s], groups[s], INT_MAX, 0, MB_HT_PASS, mins[s], uniq[s], s, nullptr};
     } else if (group_by) {
       // an absent probe contributes group value 0 (BlockSetValue, GPUProcessing.h:94-96)
       bias += static_cast<int>(static_cast<unsigned>(0 - mins[s]) * static_cast<unsigned>(uniq[s]));
@@ -280,8 +308,9 @@ static int engine_star(const int* gpuCache, const mb_filterArgsGPU* fargs, const
     a.res_layout = MB_RES_ENGINE6;
     a.res = res;
   } else {
-    // aggr1 * aggr2 summed into the u64 at res[4] (GPUProcessing.h:1757-1775)
-    if (!gargs->aggr_idx1 || !gargs->aggr_idx2) return MB_ERR_ARG;
+    // aggr1 * aggr2 summed into the u64 at res[4] (GPUProcessing.h:1757-1775); a missing
+    // column reads as 0 (BlockSetValue), so every product is 0 and nothing is added
+    if (!gargs->aggr_idx1 || !gargs->aggr_idx2) return MB_OK;
     a.aggr[0] = gargs->aggr_idx1;
     a.aggr[1] = gargs->aggr_idx2;
     a.agg_op = MB_AGG_MUL;
@@ -302,18 +331,71 @@ static int engine_star(const int* gpuCache, const mb_filterArgsGPU* fargs, const
 int mb_filter_probe_group_by_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_probeArgsGPU* pargs,
                                   const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, int start_offset,
                                   const short* segment_group, mb_stream_t stream) {
-  return engine_star(gpuCache, fargs, pargs, gargs, num_tuples, res, start_offset, segment_group, stream, true, false);
+  if (pargs == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, nullptr, fargs, pargs, gargs, num_tuples, res, start_offset, segment_group, stream,
+                     true, false);
 }
 
 int mb_probe_group_by_GPU2(const int* gpuCache, const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs,
                            int num_tuples, int* res, int start_offset, const short* segment_group, mb_stream_t stream) {
-  return engine_star(gpuCache, nullptr, pargs, gargs, num_tuples, res, start_offset, segment_group, stream, true, false);
+  if (pargs == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, nullptr, nullptr, pargs, gargs, num_tuples, res, start_offset, segment_group, stream,
+                     true, false);
 }
 
 int mb_filter_probe_aggr_GPU2(const int* gpuCache, const mb_filterArgsGPU* fargs, const mb_probeArgsGPU* pargs,
                               const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, int start_offset,
                               const short* segment_group, mb_stream_t stream) {
-  return engine_star(gpuCache, fargs, pargs, gargs, num_tuples, res, start_offset, segment_group, stream, false, true);
+  if (pargs == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, nullptr, fargs, pargs, gargs, num_tuples, res, start_offset, segment_group, stream,
+                     false, true);
+}
+
+int mb_probe_aggr_GPU2(const int* gpuCache, const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs,
+                       int num_tuples, int* res, int start_offset, const short* segment_group, mb_stream_t stream) {
+  if (pargs == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, nullptr, nullptr, pargs, gargs, num_tuples, res, start_offset, segment_group, stream,
+                     false, true);
+}
+
+int mb_filter_probe_group_by_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_filterArgsGPU* fargs,
+                                  const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs, int num_tuples,
+                                  int* res, mb_stream_t stream) {
+  if (offset == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, offset, fargs, pargs, gargs, num_tuples, res, 0, nullptr, stream, true, false);
+}
+
+int mb_probe_group_by_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_probeArgsGPU* pargs,
+                           const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, mb_stream_t stream) {
+  if (offset == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, offset, nullptr, pargs, gargs, num_tuples, res, 0, nullptr, stream, true, false);
+}
+
+int mb_groupByGPU(const int* gpuCache, const mb_offsetGPU* offset, const mb_groupbyArgsGPU* gargs, int num_tuples,
+                  int* res, mb_stream_t stream) {
+  if (offset == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, offset, nullptr, nullptr, gargs, num_tuples, res, 0, nullptr, stream, true, false);
+}
+
+int mb_aggregationGPU(const int* gpuCache, const int* lo_off, const mb_groupbyArgsGPU* gargs, int num_tuples,
+                      int* res, mb_stream_t stream) {
+  mb_offsetGPU off = {const_cast<int*>(lo_off), nullptr, nullptr, nullptr, nullptr};
+  if (lo_off == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, &off, nullptr, nullptr, gargs, num_tuples, res, 0, nullptr, stream, false, false);
+}
+
+int mb_probe_aggr_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_probeArgsGPU* pargs,
+                       const mb_groupbyArgsGPU* gargs, int num_tuples, int* res, mb_stream_t stream) {
+  if (offset == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, offset, nullptr, pargs, gargs, num_tuples, res, 0, nullptr, stream, false, true);
+}
+
+int mb_filter_probe_aggr_GPU3(const int* gpuCache, const mb_offsetGPU* offset, const mb_filterArgsGPU* fargs,
+                              const mb_probeArgsGPU* pargs, const mb_groupbyArgsGPU* gargs, int num_tuples, int* res,
+                              mb_stream_t stream) {
+  if (offset == nullptr) return MB_ERR_ARG;
+  return engine_star(gpuCache, offset, fargs, pargs, gargs, num_tuples, res, 0, nullptr, stream, false, true,
+                     kEngineSecondFilter);
 }
 
 // ---- generator ----------------------------------------------------------------------------

@@ -345,3 +345,133 @@ extern "C" int mb_cpu_star_query(const mb_star_args* a, const int* rows, int64_t
   if (status) *status |= st;
   return MB_OK;
 }
+
+// Selection with compaction on the host: the rows of the call (virtual rows, or the listed
+// ones) passing a's filters and probes, as an offset list in row order — the CPU operators
+// filter_CPU / filter_probe_CPU / probe_CPU and their list forms (CPUProcessing.cu:3-437,
+// 1158-1333). lo_off[k] = physical row; dim_off[p] (optional) = probe p's output: the
+// dimension row ht[2h+1] - 1 (VAL_OFF), the payload (KEY_VAL) or 0 (KEY). This is the CPU
+// half of a split query whose aggregation runs on the GPU over the list (the GPU3 forms).
+extern "C" int mb_cpu_star_select(const mb_star_args* a, const int* rows, int64_t num_listed, int* lo_off,
+                                  int* const* dim_off, int64_t capacity, int64_t* total_out, int nthreads,
+                                  unsigned int* status) {
+  if (a == nullptr || total_out == nullptr || capacity < 0) return MB_ERR_ARG;
+  if (a->gpu_cache != nullptr) return MB_ERR_ARG;
+  if (a->num_filters < 0 || a->num_filters > MB_MAX_FILTERS || a->num_probes < 0 || a->num_probes > MB_MAX_PROBES)
+    return MB_ERR_ARG;
+  if (a->segment_size < 0 || (a->segment_size > 0 && (a->segment_size & (a->segment_size - 1)) != 0))
+    return MB_ERR_ARG;
+  for (int f = 0; f < a->num_filters; ++f)
+    if (a->filter[f].col == nullptr || a->filter[f].mode < MB_FILTER_EQ || a->filter[f].mode > MB_FILTER_EQ_OR_EQ)
+      return MB_ERR_ARG;
+  for (int p = 0; p < a->num_probes; ++p)
+    if (a->probe[p].fkey == nullptr || a->probe[p].ht == nullptr || a->probe[p].num_slots <= 0 ||
+        a->probe[p].layout < MB_HT_KEY || a->probe[p].layout > MB_HT_VAL_OFF)
+      return MB_ERR_ARG;
+  const int64_t total = rows ? num_listed : a->num_rows;
+  if (total < 0) return MB_ERR_ARG;
+  *total_out = 0;
+  if (total == 0) return MB_OK;
+  if (capacity > 0 && lo_off == nullptr) return MB_ERR_ARG;
+
+  const int64_t ntasks = (total + kTaskRows - 1) / kTaskRows;
+  const int nt = threads_for(nthreads, total);
+  // per task: its survivors' physical rows and probe outputs, concatenated in task order
+  std::vector<std::vector<int>> t_rows(ntasks), t_dims(ntasks);
+  std::vector<unsigned> t_status(nt, 0);
+  std::atomic<int64_t> cursor{0};
+  const int64_t S = a->segment_size;
+  const int shift = S > 0 ? __builtin_ctzll(static_cast<unsigned long long>(S)) : 0;
+  const int np = a->num_probes;
+
+  Pool::get().run(nt, [&](int t) {
+    int64_t sel[kBatch];
+    int out[MB_MAX_PROBES][kBatch];
+    for (;;) {
+      const int64_t t0 = cursor.fetch_add(kTaskRows);
+      if (t0 >= total) break;
+      const int64_t task = t0 / kTaskRows;
+      const int64_t t1 = std::min(total, t0 + kTaskRows);
+      std::vector<int>& tr = t_rows[task];
+      std::vector<int>& td = t_dims[task];
+      for (int64_t b0 = t0; b0 < t1; b0 += kBatch) {
+        const int nb = static_cast<int>(std::min<int64_t>(kBatch, t1 - b0));
+        int ns = 0;
+        for (int i = 0; i < nb; ++i) {
+          const int64_t v = rows ? rows[b0 + i] : b0 + i;
+          int64_t r = v;
+          if (S > 0) {
+            const int64_t seg = a->segment_group ? a->segment_group[v >> shift] : (a->start_offset + v) >> shift;
+            r = (seg << shift) + (v & (S - 1));
+          }
+          sel[ns++] = r;
+        }
+        for (int f = 0; f < a->num_filters; ++f) {
+          const int* col = a->filter[f].col;
+          const int m = a->filter[f].mode, c1 = a->filter[f].c1, c2 = a->filter[f].c2;
+          int k = 0;
+          for (int i = 0; i < ns; ++i) {
+            const int64_t r = sel[i];
+            sel[k] = r;
+            k += pass_filter(col[r], m, c1, c2);
+          }
+          ns = k;
+        }
+        for (int p = 0; p < np; ++p) {
+          const mb_probe& Q = a->probe[p];
+          int k = 0;
+          for (int i = 0; i < ns; ++i) {
+            const int64_t r = sel[i];
+            const int h = wrap_sub(Q.fkey[r], Q.key_min) % Q.num_slots;
+            if (h < 0) {
+              t_status[t] |= MB_STATUS_PROBE_RANGE;
+              continue;
+            }
+            int o = 0;
+            bool hit;
+            if (Q.layout == MB_HT_KEY) {
+              hit = Q.ht[h] != 0;
+            } else {
+              const int lo32 = Q.ht[2 * static_cast<int64_t>(h)], hi32 = Q.ht[2 * static_cast<int64_t>(h) + 1];
+              if (Q.layout == MB_HT_VAL_OFF) {
+                hit = (lo32 | hi32) != 0;
+                o = hi32 - 1;
+              } else {
+                hit = (lo32 | hi32) != 0;
+                o = hi32;
+              }
+            }
+            if (!hit) continue;
+            sel[k] = r;
+            for (int q = 0; q < p; ++q) out[q][k] = out[q][i];
+            out[p][k] = o;
+            ++k;
+          }
+          ns = k;
+        }
+        for (int i = 0; i < ns; ++i) {
+          tr.push_back(static_cast<int>(sel[i]));
+          for (int p = 0; p < np; ++p) td.push_back(out[p][i]);
+        }
+      }
+    }
+  });
+  unsigned st = 0;
+  for (unsigned s : t_status) st |= s;
+  int64_t k = 0;
+  for (int64_t task = 0; task < ntasks; ++task) {
+    const std::vector<int>& tr = t_rows[task];
+    const std::vector<int>& td = t_dims[task];
+    for (size_t i = 0; i < tr.size(); ++i, ++k) {
+      if (k >= capacity) continue;
+      lo_off[k] = tr[i];
+      if (dim_off)
+        for (int p = 0; p < np; ++p)
+          if (dim_off[p]) dim_off[p][k] = td[i * np + p];
+    }
+  }
+  if (k > capacity) st |= MB_STATUS_OVERFLOW;
+  *total_out = k;
+  if (status) *status |= st;
+  return MB_OK;
+}

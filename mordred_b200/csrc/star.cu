@@ -135,6 +135,15 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   const DeviceState* ds = preset != nullptr ? preset : current_device_state(&err);
   if (ds == nullptr) return err;
 
+  // an offset-list input, or a group value passed through from an earlier join, runs the
+  // gather form of the pipeline
+  bool list_form = a->rows != nullptr;
+  for (int p = 0; p < a->num_probes; ++p) list_form = list_form || a->probe[p].layout == MB_HT_PASS;
+  if (list_form) {
+    if (count32) return MB_ERR_ARG;
+    return launch_list(a, stream, ds);
+  }
+
   StarPlan P;
   memset(&P, 0, sizeof(P));
   P.n = a->num_rows;

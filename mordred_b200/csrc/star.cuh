@@ -76,6 +76,10 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
 
 // Host: set per-device kernel attributes (dynamic shared memory opt-in).
 int star_init_device(const DeviceState& ds);
+// Host: the offset-list form of the pipeline (listq.cu): a->rows lists physical rows, or a
+// probe passes a group value through (MB_HT_PASS). Arguments are validated here.
+int launch_list(const mb_star_args* a, cudaStream_t stream, const DeviceState* ds);
+int list_init_device(const DeviceState& ds);
 // Host: the same for the batched multi-query kernel (batch.cu).
 int batch_init_device(const DeviceState& ds);
 

@@ -32,7 +32,7 @@ class OrcStarArgs(C.Structure):
                 ("agg_op", C.c_int), ("total_val", C.c_int), ("group_bias", C.c_int),
                 ("res_layout", C.c_int), ("res", C.c_void_p), ("count", C.c_void_p),
                 ("count_after", C.c_int), ("segment_group", C.c_void_p), ("start_offset", C.c_int64),
-                ("segment_size", C.c_int)]
+                ("segment_size", C.c_int), ("rows", C.c_void_p)]
 
 
 _lock = threading.Lock()
@@ -57,6 +57,10 @@ def lib() -> C.CDLL:
             l.orc_star.argtypes = [C.POINTER(OrcStarArgs), I]
             l.orc_build.restype = C.c_uint
             l.orc_build.argtypes = [P, I, I, I, P, P, I64, P, I, I, I, I64, P]
+            l.orc_build_rows.restype = C.c_uint
+            l.orc_build_rows.argtypes = [P, I, I, I, P, P, P, I64, P, I, I, I64, P, I, I]
+            l.orc_select.restype = C.c_int64
+            l.orc_select.argtypes = [C.POINTER(OrcStarArgs), P, P, I64, P]
             l.orc_q11.restype = C.c_ulonglong
             l.orc_q11.argtypes = [P, P, P, P, I64, I, I, I, I, I, I]
             l.orc_q21.restype = C.c_uint
@@ -120,9 +124,8 @@ def build_ht(filter_col, mode, c1, c2, key, val, ht, num_slots, key_min, layout,
                                layout, row_base, _p(presence)))
 
 
-def star(num_rows, filters=(), probes=(), aggr=(), agg_op=0, total_val=1, group_bias=0, res_layout=0, res=None,
-         count=None, count_after=-1, segment_group=None, start_offset=0, segment_size=0, nthreads=0) -> int:
-    """Run the generic pipeline; `res` (numpy, zeroed) is accumulated into. Returns status bits."""
+def _args(num_rows, filters=(), probes=(), aggr=(), agg_op=0, total_val=1, group_bias=0, res_layout=0, res=None,
+          count=None, count_after=-1, segment_group=None, start_offset=0, segment_size=0, rows=None) -> OrcStarArgs:
     a = OrcStarArgs()
     a.num_rows = num_rows
     a.num_filters = len(filters)
@@ -141,7 +144,38 @@ def star(num_rows, filters=(), probes=(), aggr=(), agg_op=0, total_val=1, group_
     a.segment_group = _p(segment_group)
     a.start_offset = start_offset
     a.segment_size = segment_size
-    return int(lib().orc_star(C.byref(a), nthreads))
+    a.rows = _p(rows)
+    return a
+
+
+LAYOUT_PASS = 3  # probe layout: payload = ht[fkey[k]] (a dimension column at a passed-through offset)
+
+
+def star(num_rows, nthreads=0, **kw) -> int:
+    """Run the generic pipeline; `res` (numpy, zeroed) is accumulated into. Returns status bits.
+    rows (optional, int32) lists the physical rows to visit (num_rows of them)."""
+    return int(lib().orc_star(C.byref(_args(num_rows, **kw)), nthreads))
+
+
+def select(num_rows, capacity=None, **kw):
+    """Rows passing the filters and probes, in visiting order: (lo_off, [dim_off per probe],
+    count, status bits)."""
+    a = _args(num_rows, **kw)
+    cap = num_rows if capacity is None else capacity
+    lo = np.zeros(max(cap, 1), np.int32)
+    dims = [np.zeros(max(cap, 1), np.int32) for _ in range(a.num_probes)]
+    arr = (C.c_void_p * 4)(*[d.ctypes.data for d in dims], *([None] * (4 - len(dims))))
+    st = C.c_uint(0)
+    k = int(lib().orc_select(C.byref(a), lo.ctypes.data, C.cast(arr, C.c_void_p), cap, C.byref(st)))
+    n = min(k, cap)
+    return lo[:n], [d[:n] for d in dims], k, int(st.value)
+
+
+def build_rows(filter_col, mode, c1, c2, key, val, rows, n, ht, num_slots, key_min, row_base=0, minmax=None,
+               val_min=0, val_max=0) -> int:
+    """Engine build (VAL_OFF) over the listed dimension rows or rows [0, n); see orc_build_rows."""
+    return int(lib().orc_build_rows(_p(filter_col), mode, c1, c2, _p(key), _p(val), _p(rows), n, _p(ht), num_slots,
+                                    key_min, row_base, _p(minmax), val_min, val_max))
 
 
 def merge(res_cpu: np.ndarray, res_gpu: np.ndarray, num_groups: int) -> None:

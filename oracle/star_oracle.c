@@ -81,6 +81,67 @@ typedef struct {
   unsigned* status;          /* per thread */
 } star_ctx;
 
+/* Physical row visited at position r of the call: the offset list, the segment mapping
+ * (CPUProcessing.cu:741,751) or r itself. */
+static inline int64_t visit_row(const orc_star_args* a, int64_t r) {
+  if (a->rows) return a->rows[r];
+  if (a->segment_size > 0) {
+    const int64_t S = a->segment_size;
+    const int64_t seg = a->segment_group ? (int64_t)a->segment_group[r / S] : (a->start_offset + r) / S;
+    return seg * S + r % S;
+  }
+  return r;
+}
+
+/* Filters, then probes in order, of the row at position r (physical row `row`), as
+ * filter_probe_group_by_CPU / _CPU2 (CPUProcessing.cu:723-1032). Returns 1 when the row
+ * passes; gv[p] = probe p's payload, out[p] = its selection output (VAL_OFF: the
+ * dimension row, KEY_VAL: the payload, KEY: 0, pass-through: the passed offset).
+ * *cnt counts rows per count_after. */
+static int eval_row(const orc_star_args* a, int64_t r, int64_t row, int* gv, int* out, unsigned* status,
+                    unsigned long long* cnt) {
+  for (int f = 0; f < a->num_filters; ++f) {
+    if (a->count_after == f) ++*cnt;
+    const int x = a->filter[f].col[row];
+    const int m = a->filter[f].mode, c1 = a->filter[f].c1, c2 = a->filter[f].c2;
+    const int ok = m == 1 ? (x >= c1 && x <= c2) : m == 0 ? (x == c1) : (x == c1 || x == c2);
+    if (!ok) return 0;
+  }
+  if (a->count_after >= a->num_filters) ++*cnt;
+  for (int p = 0; p < a->num_probes; ++p) {
+    const orc_probe* Q = &a->probe[p];
+    gv[p] = 0;
+    out[p] = 0;
+    if (Q->layout == ORC_LAYOUT_PASS) {
+      const int d = Q->fkey[r];
+      if (d < 0 || d >= Q->num_slots) { *status |= ORC_PROBE_RANGE; return 0; }
+      gv[p] = Q->ht[d];
+      out[p] = d;
+      continue;
+    }
+    const int h = pht_slot(Q->fkey[row], Q->num_slots, Q->key_min);
+    if (h < 0) { *status |= ORC_PROBE_RANGE; return 0; }
+    if (Q->layout == 0) {
+      if (Q->ht[h] == 0) return 0;
+    } else {
+      const int lo32 = Q->ht[2 * (int64_t)h], hi32 = Q->ht[2 * (int64_t)h + 1];
+      if (Q->layout == 2) {
+        /* engine tables: present when the 8-byte slot is nonzero; payload = group value,
+           selection output = the dimension row (ht[2h+1] - 1, BlockLibrary.cuh:9-33) */
+        if (lo32 == 0 && hi32 == 0) return 0;
+        gv[p] = lo32;
+        out[p] = hi32 - 1;
+      } else {
+        if (lo32 == 0 && hi32 == 0) return 0;
+        gv[p] = hi32;
+        out[p] = hi32;
+      }
+    }
+  }
+  if (a->count_after < 0) ++*cnt;
+  return 1;
+}
+
 static void star_range(void* vctx, int tid, int64_t lo, int64_t hi) {
   star_ctx* C = (star_ctx*)vctx;
   const orc_star_args* a = C->a;
@@ -91,37 +152,9 @@ static void star_range(void* vctx, int tid, int64_t lo, int64_t hi) {
   unsigned long long sum = 0, cnt = 0;
   unsigned status = 0;
   for (int64_t r = lo; r < hi; ++r) {
-    int64_t row = r;
-    if (a->segment_size > 0) {
-      int64_t S = a->segment_size;
-      int64_t seg = a->segment_group ? (int64_t)a->segment_group[r / S] : (a->start_offset + r) / S;
-      row = seg * S + r % S;
-    }
-    int pass = 1;
-    for (int f = 0; f < a->num_filters; ++f) {
-      if (a->count_after == f) ++cnt;
-      const int x = a->filter[f].col[row];
-      const int m = a->filter[f].mode, c1 = a->filter[f].c1, c2 = a->filter[f].c2;
-      int ok = m == 1 ? (x >= c1 && x <= c2) : m == 0 ? (x == c1) : (x == c1 || x == c2);
-      if (!ok) { pass = 0; break; }
-    }
-    if (!pass) continue;
-    if (a->count_after >= a->num_filters) ++cnt;
-    int gv[ORC_MAX_PROBES] = {0, 0, 0, 0};
-    for (int p = 0; p < a->num_probes && pass; ++p) {
-      const orc_probe* Q = &a->probe[p];
-      const int h = pht_slot(Q->fkey[row], Q->num_slots, Q->key_min);
-      if (h < 0) { status |= ORC_PROBE_RANGE; pass = 0; break; }
-      if (Q->layout == 0) {
-        if (Q->ht[h] == 0) pass = 0;
-      } else {
-        const int lo32 = Q->ht[2 * (int64_t)h], hi32 = Q->ht[2 * (int64_t)h + 1];
-        if (lo32 == 0 && hi32 == 0) pass = 0;
-        else gv[p] = Q->layout == 1 ? hi32 : lo32;
-      }
-    }
-    if (!pass) continue;
-    if (a->count_after < 0) ++cnt;
+    const int64_t row = visit_row(a, r);
+    int gv[ORC_MAX_PROBES] = {0, 0, 0, 0}, out[ORC_MAX_PROBES];
+    if (!eval_row(a, r, row, gv, out, &status, &cnt)) continue;
     const int a0 = a->aggr[0][row];
     int v;
     switch (a->agg_op) {
@@ -147,6 +180,26 @@ static void star_range(void* vctx, int tid, int64_t lo, int64_t hi) {
   C->sum[tid] = sum;
   C->cnt[tid] = cnt;
   C->status[tid] = status;
+}
+
+int64_t orc_select(const orc_star_args* a, int* lo_off, int* const* dim_off, int64_t capacity, unsigned* status) {
+  unsigned st = 0;
+  unsigned long long cnt = 0;
+  int64_t k = 0;
+  for (int64_t r = 0; r < a->num_rows; ++r) {
+    const int64_t row = visit_row(a, r);
+    int gv[ORC_MAX_PROBES], out[ORC_MAX_PROBES];
+    if (!eval_row(a, r, row, gv, out, &st, &cnt)) continue;
+    if (k < capacity) {
+      lo_off[k] = (int)row;
+      if (dim_off)
+        for (int p = 0; p < a->num_probes; ++p)
+          if (dim_off[p]) dim_off[p][k] = out[p];
+    }
+    ++k;
+  }
+  if (status) *status |= st;
+  return k;
 }
 
 unsigned orc_star(const orc_star_args* a, int nthreads) {
@@ -224,6 +277,36 @@ unsigned orc_build(const int* filter, int mode, int c1, int c2, const int* key, 
       present = 1;
     }
     if (presence && present) presence[h >> 5] |= 1u << (h & 31);
+  }
+  return status;
+}
+
+unsigned orc_build_rows(const int* filter, int mode, int c1, int c2, const int* key, const int* val,
+                        const int* rows, int64_t n, int* ht, int num_slots, int key_min, int64_t row_base,
+                        int* minmax, int val_min, int val_max) {
+  unsigned status = 0;
+  int mn = val_max, mx = val_min;  /* the reference's per-task starting values */
+  for (int64_t i = 0; i < n; ++i) {
+    /* columns are read at the listed dimension row (or at i); the stored row id is that
+       row (or row_base + i) */
+    const int64_t row = rows ? (int64_t)rows[i] : i;
+    const int64_t rowid = rows ? row : row_base + i;
+    if (filter) {
+      const int x = filter[row];
+      const int ok = mode == 1 ? (x >= c1 && x <= c2) : mode == 0 ? (x == c1) : (x == c1 || x == c2);
+      if (!ok) continue;
+    }
+    const int k = key[row];
+    if (k < mn) mn = k;
+    if (k > mx) mx = k;
+    const int h = pht_slot(k, num_slots, key_min);
+    if (h < 0) { status |= ORC_PROBE_RANGE; continue; }
+    if (val && ht[2 * (int64_t)h] == 0) ht[2 * (int64_t)h] = val[row];
+    ht[2 * (int64_t)h + 1] = (int)(rowid + 1);
+  }
+  if (minmax && n > 0) {
+    if (mn < minmax[0]) minmax[0] = mn;
+    if (mx > minmax[1]) minmax[1] = mx;
   }
   return status;
 }

@@ -31,6 +31,12 @@ extern "C" {
 
 typedef struct orc_filter { const int* col; int mode; int c1, c2; } orc_filter;
 
+/* Probe layouts 0 KEY, 1 KEY_VAL, 2 VAL_OFF as in orc_build; 3 = no table, the payload is
+ * passed through from an earlier join: payload = ht[fkey[k]] where ht is a dimension column,
+ * fkey a dimension-offset list read at list position k, num_slots the dimension's rows
+ * (CPUProcessing.cu:905-908, "dim_val1 = gargs.group_col1[offset.h_dim_off1[...]]"). */
+#define ORC_LAYOUT_PASS 3
+
 typedef struct orc_probe {
   const int* fkey;
   const int* ht;
@@ -55,10 +61,24 @@ typedef struct orc_star_args {
   const short* segment_group;
   int64_t start_offset;
   int segment_size;
+  /* Offset-list input (the *_CPU2 forms, CPUProcessing.cu:868-1032): when rows is
+   * non-NULL the call visits k in [0, num_rows) and reads every column at the physical
+   * row rows[k] (no segment mapping); pass-through probes read their lists at k. */
+  const int* rows;
 } orc_star_args;
 
 /* Returns ORC_* status bits (0 = clean). nthreads <= 0: all hardware threads. */
 unsigned orc_star(const orc_star_args* a, int nthreads);
+
+/* Selection with compaction (filter_probe_CPU / probe_CPU / filter_CPU and their list
+ * forms, CPUProcessing.cu:3-437,1158-1333): the rows passing a's filters and probes, in
+ * visiting order. lo_off[k] = physical row; dim_off[p] (optional per probe) = the probe's
+ * output: VAL_OFF the dimension row ht[2h+1] - 1, KEY_VAL the payload, KEY 0, a
+ * pass-through probe its passed offset. Writes at most `capacity` entries, returns the
+ * number of passing rows; *status (optional) receives ORC_* bits. Aggregate fields of a
+ * are ignored. Sequential. */
+int64_t orc_select(const orc_star_args* a, int* lo_off, int* const* dim_off, int64_t capacity,
+                   unsigned* status);
 
 /* Filtered PHT build into a zeroed table in `layout` (0 KEY, 1 KEY_VAL, 2 VAL_OFF).
  * filter NULL = no filter; mode 0 EQ, 1 BETWEEN, 2 EQ OR EQ. row ids for VAL_OFF are
@@ -66,6 +86,16 @@ unsigned orc_star(const orc_star_args* a, int nthreads);
 unsigned orc_build(const int* filter, int mode, int c1, int c2, const int* key, const int* val,
                    int64_t n, int* ht, int num_slots, int key_min, int layout, int64_t row_base,
                    uint32_t* presence);
+
+/* Engine builds over a dimension-offset list or with the key range (build_CPU2,
+ * build_CPU_minmax, build_CPU_minmax2: CPUProcessing.cu:1106-1156,1821-1994): rows
+ * (optional) lists the dimension rows to build from (row id = rows[k]); otherwise rows
+ * row_base + i. Layout VAL_OFF. minmax (optional, int[2]) folds in the min and max key of
+ * the rows that pass the filter, starting from {val_max, val_min} as the reference's
+ * per-task accumulators do. */
+unsigned orc_build_rows(const int* filter, int mode, int c1, int c2, const int* key, const int* val,
+                        const int* rows, int64_t n, int* ht, int num_slots, int key_min, int64_t row_base,
+                        int* minmax, int val_min, int val_max);
 
 /* src/cpu/ssb/q11.cpp:21-70 with the predicate constants as parameters. */
 unsigned long long orc_q11(const int* lo_orderdate, const int* lo_discount, const int* lo_quantity,

@@ -198,3 +198,32 @@ def test_batch_graph_replay_and_autotune():
         assert torch.equal(a.view(-1), b.view(-1))
     del g
     assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
+def test_batch_256_mixed_against_oracle():
+    """Every query of a 256-query mixed batch (filter-aggregate, Query A, Query B forms;
+    group counts 1, 175 and 7,000) against the CPU oracle running it alone with filtered
+    tables — the pin for the batched kernel, not another CUDA run."""
+    import torch
+    from mordred_b200 import _lib as L
+    from query_oracle import expected
+    torch.cuda.set_device(0)
+    n = 2_000_003
+    s = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(s, 2027, B.BATCH_FACT, B.BATCH_DIMS)
+    pats = B.build_pats(t, s)
+    qs = B.generate_queries(256, seed=99, sel_lo=1e-4, sel_hi=0.3)
+    flat, views = B.result_buffers(qs)
+    B.BatchPlan(t, pats, qs, views, n).run()
+    torch.cuda.synchronize()
+    h = {k: v.cpu().numpy() for k, v in t.items()}
+    nonempty = 0
+    for i, q in enumerate(qs):
+        exp = expected(h, s, q)
+        got = views[i].cpu().numpy().reshape(-1)
+        assert np.array_equal(got, exp), (i, q.template)
+        nonempty += bool(np.any(exp != 0))
+    assert nonempty > 200
+    assert {q.template for q in qs} == {"agg", "qa", "qb"}
+    assert L.device_status(0) == 0

@@ -33,7 +33,7 @@ def status():
 
 # ---- filter-aggregate (q11 form) ---------------------------------------------------------
 
-@pytest.mark.parametrize("n", [0, 1, 5, 2047, 2048, 2049, 8191, 196_625, 1_000_003])
+@pytest.mark.parametrize("n", [0, 1, 5, 2047, 2048, 2049, 8191, 196_625, 1_000_003, 6_000_000])
 def test_q11_parity(n):
     s = ssb.Sizes(lo_len=n)
     t = ssb.gen_device(s, 100 + n, ssb.Q11_COLUMNS, [])
