@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-planner", action="store_true")
     ap.add_argument("--planner-rows", type=int, default=600_000_000)
-    ap.add_argument("--planner-queries", type=int, default=300)
+    ap.add_argument("--planner-queries", type=int, default=2000)
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-rows", type=int, default=600_000_000)
@@ -169,6 +169,98 @@ def cpu_baseline_port(rows: int, trials: int):
     return steps, os.cpu_count() or 1
 
 
+def filter_aggregate_full(t, n, ws, reps=20):
+    """Median CUDA-event time of the filter-aggregate over the whole resident table."""
+    import torch
+
+    from mordred_b200 import ssb
+
+    ms = []
+    for _ in range(reps + 2):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ssb.q11(t, n, ws, zero=False)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    return statistics.median(ms[2:])
+
+
+def filter_aggregate_6m(s, rank, peak, copies=20, rows=6_000_000, reps=10):
+    """Config 1: the filter-aggregate on 6,000,000-row tables, each launch reading a table of
+    its own (copies x 96 MB, larger than L2 together) in a CUDA graph of back-to-back
+    launches; results checked against the first direct run of each copy."""
+    import torch
+
+    from mordred_b200 import _lib as L
+    from mordred_b200 import ssb
+
+    st = ssb._stream()
+    tabs = []
+    for k in range(copies):
+        tk = {}
+        for name in ssb.Q11_COLUMNS:
+            buf = torch.empty(rows, dtype=torch.int32, device="cuda")
+            L.call("mb_gen_fact_column", ssb.FACT_COLUMNS[name], SEED + 1000 + k, rank * rows, rows, s.s_len, s.c_len,
+                   s.p_len, ssb._p(buf), st)
+            tk[name] = buf
+        tabs.append(tk)
+    rev = torch.zeros(copies, dtype=torch.int64, device="cuda")
+    cnt = torch.zeros(copies, dtype=torch.int32, device="cuda")
+
+    def launch_all():
+        for k, tk in enumerate(tabs):
+            L.call("mb_q11_query", ssb._p(tk["lo_orderdate"]), ssb._p(tk["lo_discount"]), ssb._p(tk["lo_quantity"]),
+                   ssb._p(tk["lo_extendedprice"]), rows, rev[k:].data_ptr(), cnt[k:].data_ptr(), ssb._stream())
+
+    launch_all()
+    torch.cuda.synchronize()
+    first = rev.clone()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        rev.zero_()
+        cnt.zero_()
+        launch_all()
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    equal = bool(torch.equal(rev, first))
+    per_launch = e0.elapsed_time(e1) / (reps * copies)
+    # the same launches one by one, each after a 512 MB write and a 512 MB read of other
+    # buffers (cold L2): the latency of one query on its own, launch overhead included
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    clean = torch.ones(128 << 20, dtype=torch.int32, device="cuda")
+    sink = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cold = []
+    for k in range(min(copies, 12)):
+        flush.zero_()
+        sink.add_(clean.sum(dtype=torch.int64))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        L.call("mb_q11_query", ssb._p(tabs[k]["lo_orderdate"]), ssb._p(tabs[k]["lo_discount"]),
+               ssb._p(tabs[k]["lo_quantity"]), ssb._p(tabs[k]["lo_extendedprice"]), rows, rev[k:].data_ptr(),
+               cnt[k:].data_ptr(), ssb._stream())
+        b.record()
+        torch.cuda.synchronize()
+        cold.append(a.elapsed_time(b))
+    del g, flush, clean, tabs
+    torch.cuda.empty_cache()
+    gbs = rows * 16 / per_launch / 1e6
+    cold_ms = statistics.median(cold[2:])
+    return {"rows": rows, "ms": per_launch, "fact_rows_per_s": rows / (per_launch / 1e3), "gbs": gbs,
+            "frac_of_hbm": gbs / peak, "results_equal_direct_run": equal,
+            "l2": f"{copies} separate {rows:,}-row tables ({copies * rows * 16 / 1e9:.2f} GB) in turn, CUDA graph of "
+                  f"{copies} back-to-back launches, {reps} replays",
+            "cold_single_launch": {"ms": cold_ms, "frac_of_hbm": rows * 16 / cold_ms / 1e6 / peak,
+                                   "l2": "512 MB write then 512 MB read of other buffers before each launch"}}
+
+
 def batch_section(t, s, n, rank, world, args):
     """256 generated queries (filter-aggregate, Query A and Query B forms; selectivities
     log-uniform in [1e-5, 0.3]) over this rank's fact rows: one batched scan, replayed
@@ -242,15 +334,21 @@ def batch_section(t, s, n, rank, world, args):
 
 
 def planner_section(args):
-    """Learned vs analytic planner over a host-resident, date-sorted fact table of
-    --planner-rows rows (1 Mi-row segments, per-segment min/max) with an 8 GB GPU segment
-    cache: the same generated queries run under each planner from the same starting
-    cache (CPU and GPU shares concurrent, results compared bit for bit); plus the mean
-    absolute error of each model's log-ms predictions on segments profiled live here."""
+    """Config 3: a host-resident, date-sorted fact table of --planner-rows rows (1 Mi-row
+    segments, per-segment min/max) under an 8 GB GPU segment-cache budget, and
+    --planner-queries generated queries. The plain form runs them one at a time (the
+    reference's executor) with the analytic cost model and with the learned model; the
+    batched form runs them in windows of 256 through the batched executor (shared scans,
+    planner-driven placement and admission, staged streaming) with each model. Every form
+    starts from the same cache contents; results are compared bit for bit across forms.
+    Plus the mean absolute error of each model's log-ms predictions on segments profiled
+    live here, and on the training log's hold-out."""
     import numpy as np
+    import torch
 
     from mordred_b200 import batch as B
     from mordred_b200 import planner_experiment as PE
+    from mordred_b200.batch_engine import BatchExecutor
     from mordred_b200.engine import SEG, Executor, SegmentedTable
     from mordred_b200.planner import MIN_MS, AnalyticPlanner, LearnedPlanner
 
@@ -259,11 +357,14 @@ def planner_section(args):
     learned = LearnedPlanner.load(PE.DEFAULT_WEIGHTS)
     t0 = time.perf_counter()
     table = SegmentedTable(args.planner_rows, SEED)
-    ex = Executor(table, cache_slots=int(8 * (1 << 30) // (SEG * 4)))
+    slots = int(8 * (1 << 30) // (SEG * 4))
     setup_s = time.perf_counter() - t0
     queries = B.generate_queries(args.planner_queries, seed=SEED + 7)
-    ev = PE.evaluate(ex, [AnalyticPlanner(), learned], queries, PE.initial_weights(table, queries),
-                     log=lambda *a: None)
+    start = PE.initial_weights(table, queries)
+    plain_res, batch_res = {}, {}
+    ex = Executor(table, cache_slots=slots)
+    plain = PE.evaluate(ex, [AnalyticPlanner(), learned], queries, start, log=lambda *a: None,
+                        keep_results=plain_res)
     # live prediction error on freshly profiled segments (a different query seed)
     rng = np.random.default_rng(SEED + 11)
     feats, truth, ana = [], [], []
@@ -280,13 +381,30 @@ def planner_section(args):
     live = {"samples": len(feats),
             "learned": PE.mae_report(learned.predict_log(np.stack(feats)), truth),
             "analytic": PE.mae_report(np.log(np.maximum(np.array(ana), MIN_MS)), truth)}
-    return {"fact_rows": args.planner_rows, "segments": table.nseg, "cache_slots": ex.cache.num_slots,
+    ex.cache.close()
+    del ex
+    torch.cuda.empty_cache()
+    bx = BatchExecutor(table, cache_slots=slots)
+    batched = PE.evaluate_batched(bx, [AnalyticPlanner(), learned], queries, start, log=lambda *a: None,
+                                  keep_results=batch_res)
+    bx.cache.close()
+    del bx
+    torch.cuda.empty_cache()
+    ref = plain_res["analytic"]
+    identical = all(all(np.array_equal(a, b) for a, b in zip(ref, r)) for r in
+                    [plain_res["learned"], batch_res["analytic"], batch_res["learned"]])
+    base = plain["analytic"]["total_ms"]
+    return {"fact_rows": args.planner_rows, "segments": table.nseg, "cache_slots": slots,
             "queries": len(queries), "setup_s": setup_s,
-            "learned_ms": ev["learned"]["total_ms"], "analytic_ms": ev["analytic"]["total_ms"],
-            "speedup_learned_vs_analytic": ev["analytic"]["total_ms"] / ev["learned"]["total_ms"],
-            "per_planner": {k: ev[k] for k in ("analytic", "learned")},
-            "results_identical": ev["results_identical"], "prediction_mae_live": live,
-            "prediction_mae_training_holdout": learned.manifest.get("holdout"),
+            "plain_analytic_ms": base, "plain_learned_ms": plain["learned"]["total_ms"],
+            "batched_analytic_ms": batched["analytic"]["total_ms"],
+            "batched_learned_ms": batched["learned"]["total_ms"],
+            "speedup_batched_learned_vs_plain_analytic": base / batched["learned"]["total_ms"],
+            "speedup_learned_vs_analytic_plain": base / plain["learned"]["total_ms"],
+            "speedup_learned_vs_analytic_batched": batched["analytic"]["total_ms"] / batched["learned"]["total_ms"],
+            "one_at_a_time": {k: plain[k] for k in ("analytic", "learned")},
+            "batched": batched, "results_identical_all_forms": identical,
+            "prediction_mae_live": live, "prediction_mae_training_holdout": learned.manifest.get("holdout"),
             "weights": "mordred_b200/planner_weights/mlp.bin", "seed": SEED}
 
 
@@ -319,6 +437,29 @@ def serve_section(args):
                                                           "mean_batch", "mean_batch_ms")})
     del whole, circ, t
     torch.cuda.empty_cache()
+    return out
+
+
+def summary_of(per_query, batched, planner, serving) -> dict:
+    """The headline figure of each section, so that the end of the line carries them all."""
+    out = {"filter_aggregate_6M_frac_of_hbm": per_query["filter_aggregate_6M"].get("frac_of_hbm"),
+           "query_a_frac_of_hbm": per_query["A"]["frac_of_hbm"], "query_b_frac_of_hbm": per_query["B"]["frac_of_hbm"]}
+    if batched:
+        out["batched_256_ms"] = batched["batched_ms"]
+        out["batched_vs_one_at_a_time"] = batched["speedup"]
+        out["batched_results_equal"] = batched["results_equal_one_at_a_time"]
+    if planner and "plain_analytic_ms" in planner:
+        out["config3_queries"] = planner["queries"]
+        for k in ("plain_analytic_ms", "plain_learned_ms", "batched_analytic_ms", "batched_learned_ms",
+                  "speedup_batched_learned_vs_plain_analytic", "results_identical_all_forms"):
+            out["config3_" + k] = planner[k]
+        live = planner["prediction_mae_live"]
+        out["config3_mae_log_ms_learned"] = live["learned"]["mae_log_ms"]
+        out["config3_mae_log_ms_analytic"] = live["analytic"]["mae_log_ms"]
+    if serving:
+        out["serving_qps"] = serving.get("qps")
+        out["serving_p50_ms"] = serving.get("p50_ms")
+        out["serving_p99_ms"] = serving.get("p99_ms")
     return out
 
 
@@ -461,32 +602,13 @@ def main():
         if k:
             traffic = k["bytes_per_launch_scaled"]
 
-    # ---- filter-aggregate (16 B/row): the full table, and the 6 M-row table of its own
-    # workload (96 MB, inside L2). Before every timed launch of the small table a 512 MB
-    # write flushes L2 and a 512 MB read of another buffer then evicts the written lines,
-    # so the launch starts cold and does not pay the flush's write-backs -----------------
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    clean = torch.ones(128 << 20, dtype=torch.int32, device="cuda")
-    sink = torch.zeros(1, dtype=torch.int64, device="cuda")
-
-    def time_q11(rows, reps, do_flush):
-        ms = []
-        for _ in range(reps + 2):
-            if do_flush:
-                flush.zero_()
-                sink.add_(clean.sum(dtype=torch.int64))
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            ssb.q11(t, rows, ws, zero=False)
-            b.record()
-            torch.cuda.synchronize()
-            ms.append(a.elapsed_time(b))
-        return statistics.median(ms[2:])
-
-    f_full = time_q11(n, 20, False)
-    f_small_rows = min(n, 6_000_000)
-    f_small = time_q11(f_small_rows, 20, True)
-    del flush, clean
+    # ---- filter-aggregate (16 B/row) on the full table, and on config 1's own 6 M-row table:
+    # 20 separate 6 M-row copies (1.92 GB, far above L2) launched back to back from a CUDA
+    # graph, so every launch reads its table from HBM with no flush inside the timed
+    # region; per-launch time = replay time / 20. The old cold single launch (a 512 MB write
+    # and a 512 MB read of other buffers before it) is reported beside it --------------------
+    f_full = filter_aggregate_full(t, n, ws)
+    f_small = filter_aggregate_6m(s, rank, peak)
 
     # ---- batched multi-query execution: 256 queries over the same fact rows ---------------
     batched = None if args.no_batch else batch_section(t, s, n, rank, world, args)
@@ -550,36 +672,35 @@ def main():
                "ms_per_step": cms}
 
     if rank == 0:
+        per_query = {
+            "filter_aggregate_6M": f_small,
+            "filter_aggregate": {"ms": f_full, "fact_rows_per_s": n / (f_full / 1e3),
+                                 "gbs": n * 16 / f_full / 1e6, "frac_of_hbm": n * 16 / f_full / 1e6 / peak},
+            "A": {"probe_ms": pa, "fact_rows_per_s": n / (pa / 1e3), "gbs": n * QA_BYTES_PER_ROW / pa / 1e6,
+                  "frac_of_hbm": n * QA_BYTES_PER_ROW / pa / 1e6 / peak},
+            "B": {"probe_ms": pb, "fact_rows_per_s": n / (pb / 1e3), "gbs": n * QB_BYTES_PER_ROW / pb / 1e6,
+                  "frac_of_hbm": n * QB_BYTES_PER_ROW / pb / 1e6 / peak},
+        }
+        # the long sections first; the line ends with the headline figures of every section
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32 (int64 sums)", "data": "synthetic",
             "config": workload_config(n, s, world),
-            "per_query": {
-                "filter_aggregate": {"ms": f_full, "fact_rows_per_s": n / (f_full / 1e3),
-                                     "gbs": n * 16 / f_full / 1e6, "frac_of_hbm": n * 16 / f_full / 1e6 / peak},
-                "filter_aggregate_6M": {"rows": f_small_rows, "ms": f_small,
-                                        "fact_rows_per_s": f_small_rows / (f_small / 1e3),
-                                        "gbs": f_small_rows * 16 / f_small / 1e6,
-                                        "frac_of_hbm": f_small_rows * 16 / f_small / 1e6 / peak,
-                                        "l2": "512 MB write then 512 MB read of another buffer before each "
-                                              "launch (cold L2, no dirty lines left)"},
-                "A": {"probe_ms": pa, "fact_rows_per_s": n / (pa / 1e3), "gbs": n * QA_BYTES_PER_ROW / pa / 1e6,
-                      "frac_of_hbm": n * QA_BYTES_PER_ROW / pa / 1e6 / peak},
-                "B": {"probe_ms": pb, "fact_rows_per_s": n / (pb / 1e3), "gbs": n * QB_BYTES_PER_ROW / pb / 1e6,
-                      "frac_of_hbm": n * QB_BYTES_PER_ROW / pb / 1e6 / peak},
-            },
-            "roofline": {"bound": "hbm", "kernel": f"star_kernel (Query {dom} probe)", "achieved": achieved,
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": bytes_dom},
-            "batched": batched,
             "planner": planner if world == 1 else {"skipped": "the planner experiment runs at N = 1"},
             "serving": serving if world == 1 else {"skipped": "the serving loop runs at N = 1"},
+            "batched": batched,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "device_status": status,
+            "roofline": {"bound": "hbm", "kernel": f"star_kernel (Query {dom} probe)", "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": bytes_dom},
+            "per_query": per_query,
+            "summary": summary_of(per_query, batched, planner if world == 1 else None,
+                                  serving if world == 1 else None),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -387,6 +387,14 @@ typedef struct mb_batch_args {
    * 960x1 (0 = default 768x1); stages 2..8 (0 = 2); grid 0 = one CTA per SM */
   int threads, items_per_thread, stages, grid;
   int smem_group_bytes;                   /* shared memory for small group arrays; -1 default, 0 none */
+  /* Segment-cache addressing (optional; src/gpudb/GPUProcessing.h:54-67 for one query):
+   * when gpu_cache is non-NULL, fact[c] is column c's per-segment cache-slot array and row r
+   * of the batch reads gpu_cache[slot * segment_size + r % segment_size], slot =
+   * fact[c][segment_group[r / segment_size]] (r / segment_size without a list). One launch
+   * thus scans a list of cached or staged segments for every query of the batch. */
+  const int* gpu_cache;
+  const short* segment_group;
+  int segment_size;                       /* power of two */
 } mb_batch_args;
 
 /* Build a PAT: for each dimension row i, words[(key[i] - key_min) % slots] =
@@ -591,6 +599,17 @@ int mb_segcache_evict(mb_segcache* cache, int col, int seg);
 int mb_segcache_replace(mb_segcache* cache, const double* weights, const int* const* host_cols,
                         const int* segment_rows, mb_stream_t stream);
 int mb_segcache_get_stats(mb_segcache* cache, mb_segcache_stats* out);
+/* Take the nslots highest slots not yet reserved out of the cache's management (evicting
+ * what they hold): admission and replacement never use them again, and the caller owns
+ * them — a staging area for segments it streams through the pool without making them
+ * resident (slot s at mb_segcache_pool() + s * segment_size). *first_slot = the lowest
+ * reserved slot. MB_ERR_SIZE when no managed slot would be left. No counterpart in the
+ * reference, whose executor admits every segment it reads. */
+int mb_segcache_reserve(mb_segcache* cache, int64_t nslots, int64_t* first_slot);
+/* Copy `rows` ints from host_src (pinned for an asynchronous copy) into reserved slot
+ * `slot` on `stream`; the slot's map entry is the caller's to keep. MB_ERR_ARG for a slot
+ * the cache manages. */
+int mb_segcache_stage(mb_segcache* cache, int64_t slot, const int* host_src, int rows, mb_stream_t stream);
 
 /* ---- synthetic data (seeded; identical on host and device) ---------------------- */
 /* Fact column `col` (MB_LO_* in mordred_b200/csrc/ssbgen.h) rows [row0, row0+n) into a

@@ -202,7 +202,8 @@ class MbBatchArgs(C.Structure):
     _fields_ = [("num_rows", C.c_int64), ("fact", C.c_void_p * MB_NUM_FACT_COLS), ("dim", MbPat * 4),
                 ("num_queries", C.c_int), ("queries", C.POINTER(MbBatchQuery)), ("workspace", C.c_void_p),
                 ("workspace_bytes", C.c_size_t), ("threads", C.c_int), ("items_per_thread", C.c_int),
-                ("stages", C.c_int), ("grid", C.c_int), ("smem_group_bytes", C.c_int)]
+                ("stages", C.c_int), ("grid", C.c_int), ("smem_group_bytes", C.c_int),
+                ("gpu_cache", C.c_void_p), ("segment_group", C.c_void_p), ("segment_size", C.c_int)]
 
 
 MB_CACHE_LRU, MB_CACHE_LFU, MB_CACHE_WEIGHT = 0, 1, 2
@@ -267,6 +268,8 @@ SIGNATURES.update({
     "mb_segcache_admit_segments": (I, [P, P, I, P, I, P, P, P, PS(I), PS(C.c_ulonglong)]),
     "mb_segcache_replace": (I, [P, P, P, P, P]),
     "mb_segcache_get_stats": (I, [P, PS(MbSegcacheStats)]),
+    "mb_segcache_reserve": (I, [P, I64, PS(C.c_int64)]),
+    "mb_segcache_stage": (I, [P, I64, P, I, P]),
     "mb_cpu_threads": (I, []),
     "mb_cpu_build_pht": (I, [P, I, I, I, P, P, I, P, I, I, I, I, PS(C.c_uint)]),
     "mb_cpu_star_query": (I, [PS(MbStarArgs), P, I64, I, PS(C.c_uint)]),

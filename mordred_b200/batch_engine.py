@@ -1,0 +1,287 @@
+"""Batched execution over the host-resident segmented table: a window of queued queries is
+answered by shared scans, with the planner deciding which segments the GPU scans for all
+of them and which the host cores run per query, and which column segments stay resident
+in the GPU segment cache.
+
+The reference runs one query at a time (src/gpudb/QueryProcessing.cu:1347-1471), placing
+each query's segment groups on a device from the cost model (QueryOptimizer.cu:1674-1891)
+and refilling its segment cache by benefit weights (CacheManager.cu:534-588). Here:
+
+* candidates — per query, the segments whose orderdate range meets the query's
+  (QueryOptimizer.cu:1641-1662); the window's union is what the GPU may have to scan.
+* placement — the planner (learned MLP or the analytic model) predicts, per (query,
+  candidate segment), CPU ms and GPU ms. A segment's GPU cost in the batch is the most
+  expensive member's (the copies of its columns and the scan are shared by every query
+  of the window); its CPU cost is the sum over the queries that need it, each with its
+  share of that query's host hash-table builds. mb_place_segments splits the union to
+  minimise the window's makespan.
+* admission — every window the planner's predicted saving from residency (GPU ms with
+  the segment's columns missing minus resident, per column) of each column segment the
+  window reads is added into an exponentially weighted benefit, and the cache keeps the
+  heaviest (mb_segcache_replace, the reference's SegmentReplacement with the model's
+  weights). Segments the GPU scans that are not resident stream through reserved
+  staging slots (mb_segcache_reserve / mb_segcache_stage) without evicting anything.
+* execution — resident segments are scanned at once; staged segments go in waves,
+  copies of wave w + 1 on a copy stream overlapping the scan of wave w on the kernel
+  stream (two staging buffers); every scan is one batched launch (mb_batch_run with
+  segment-cache addressing) per 256 queries. The host share runs concurrently on the
+  CPU engine. Each query's GPU and CPU partial results merge by addition
+  (CPUProcessing.cu:1786-1819).
+Results equal each query run alone (integer sums; tests/test_batch_engine.py).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import batch as B
+from . import cpu, ssb
+from .engine import COL_ID, FACT, NEEDED, SEG, CpuShare, SegmentedTable, host_tables, merge
+from .planner import place
+from .segcache import SegmentCache
+
+
+@dataclass
+class WindowRun:
+    """Outcome of one window: per-query merged results (host) and timings."""
+    results: list
+    ms: float
+    queries: int
+    union_segments: int
+    gpu_segments: int
+    cpu_segments: int
+    staged_segments: int
+    launches: int
+    predicted_makespan_ms: float
+    plan_ms: float = 0.0
+    gpu_ms: float = 0.0
+    cpu_ms: float = 0.0
+    copied_column_segments: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+class BatchExecutor(CpuShare):
+    """Windows of queries over a :class:`SegmentedTable` with a GPU segment cache of
+    `cache_slots` slots (the budget includes the staging slots)."""
+
+    def __init__(self, table: SegmentedTable, cache_slots: int = 2048, stage_segments: int = 12, device: int = 0,
+                 benefit_decay: float = 0.5):
+        ncol = len(FACT)
+        self.t = table
+        self.cache = SegmentCache(cache_slots, SEG, ncol, table.nseg, "weight", device)
+        self.stage_segments = stage_segments
+        self.stage0 = self.cache.reserve(2 * stage_segments * ncol)
+        self.hht = host_tables(table.sizes)
+        self.cpu_threads = cpu.threads()
+        dims = dict(table.dims)
+        extra = [d for d in B.BATCH_DIMS if d not in dims]
+        dims.update(ssb.gen_device(table.sizes, table.seed, [], extra))
+        self.dims = dims
+        self.pats = B.build_pats(dims, table.sizes)
+        self.c_dims = self.pats.c_dims()
+        self.kstream = torch.cuda.Stream()
+        self.cstream = torch.cuda.Stream()
+        self.max_waves = table.nseg // stage_segments + 3
+        self.col_h = torch.empty(self.max_waves, ncol, table.nseg, dtype=torch.int32, pin_memory=True)
+        self.col_d = torch.empty(self.max_waves, ncol, table.nseg, dtype=torch.int32, device="cuda")
+        self.seg_h = torch.empty(self.max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
+        self.seg_d = torch.empty(self.max_waves, table.nseg, dtype=torch.int16, device="cuda")
+        self.ws = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
+        self.host_ptrs = [table.ptr(c, 0) for c in FACT]
+        self.benefit = np.zeros((ncol, table.nseg))
+        self.decay = benefit_decay
+        self.admission = True
+
+    # ---- planning ------------------------------------------------------------------------
+    def _predict(self, planner, queries, cands):
+        """Per query: (cpu_ms, gpu_ms, cpu_fixed, gpu_fixed, gpu_ms if missing, gpu_ms if
+        resident) over its candidate segments, from one batched model call."""
+        ctxs = [self.context(q, c) for q, c in zip(queries, cands)]
+        base = planner.predict_many(ctxs)
+        if not self.admission:
+            return base, None
+        lo, hi = [], []
+        for ctx in ctxs:
+            a = ctx.subset(slice(None))
+            a.resident_cols = np.zeros_like(ctx.resident_cols)
+            b = ctx.subset(slice(None))
+            b.resident_cols = np.full_like(ctx.resident_cols, ctx.needed_cols)
+            lo.append(a)
+            hi.append(b)
+        miss = planner.predict_many(lo)
+        res = planner.predict_many(hi)
+        saving = [np.maximum(m[1] - r[1], 0.0) for m, r in zip(miss, res)]
+        return base, saving
+
+    def _admit(self, queries, cands, saving, stream) -> int:
+        """Fold this window's predicted residency savings into the benefit weights and
+        replace the cache's contents by them; returns the column segments copied in."""
+        win = np.zeros_like(self.benefit)
+        for q, cand, sv in zip(queries, cands, saving):
+            cols = [COL_ID[c] for c in NEEDED[q.template]]
+            if len(cand) == 0:
+                continue
+            for c in cols:
+                win[c, cand] += sv / len(cols)
+        self.benefit = self.decay * self.benefit + win
+        before = self.cache.stats()["admissions"]
+        with torch.cuda.stream(stream):
+            self.cache.replace(self.benefit, self.host_ptrs, self.t.seg_rows, stream.cuda_stream)
+        return self.cache.stats()["admissions"] - before
+
+    # ---- GPU share -------------------------------------------------------------------------
+    def _launch(self, w: int, segs: np.ndarray, qarrs: list, cols_needed: list[int], stream) -> int:
+        """One batched launch per chunk of up to 256 queries over the wave's segments
+        (col_d[w] / seg_d[w] already hold its slot arrays); returns launches issued."""
+        n_rows = self._rows(segs)
+        launches = 0
+        for arr, nq, cols in qarrs:
+            a = L.MbBatchArgs()
+            a.num_rows = n_rows
+            for c in cols:
+                a.fact[c] = self.col_d[w, c].data_ptr()
+            a.dim = self.c_dims
+            a.num_queries = nq
+            a.queries = C.cast(arr, C.POINTER(L.MbBatchQuery))
+            a.smem_group_bytes = -1
+            a.gpu_cache = self.cache.pool
+            a.segment_group = self.seg_d[w].data_ptr()
+            a.segment_size = SEG
+            need = int(L.lib().mb_batch_workspace_bytes(C.byref(a)))
+            if need > self.ws.numel():
+                stream.synchronize()
+                self.ws = torch.empty(2 * need, dtype=torch.uint8, device="cuda")
+            a.workspace, a.workspace_bytes = self.ws.data_ptr(), self.ws.numel()
+            L.check("mb_batch_run", L.lib().mb_batch_run(C.byref(a), stream.cuda_stream))
+            launches += 1
+        return launches
+
+    def _gpu_share(self, gsegs: np.ndarray, qarrs, cols_needed: list[int]) -> tuple[int, int, int]:
+        """Scan gsegs for every query: resident segments in one launch, the others staged
+        in waves; returns (launches, waves, column segments staged)."""
+        ks, cs = self.kstream, self.cstream
+        if len(gsegs) == 0:
+            return 0, 0, 0
+        idx = {c: self.cache.col_idx(c) for c in cols_needed}
+        resident = np.array([all(idx[c][s] >= 0 for c in cols_needed) for s in gsegs], bool)
+        waves = []
+        if resident.any():
+            waves.append((self._order(gsegs[resident], self.t), False))
+        rest = gsegs[~resident]
+        for i in range(0, len(rest), self.stage_segments):
+            waves.append((self._order(rest[i: i + self.stage_segments], self.t), True))
+        launches, staged = 0, 0
+        done_ev = [None, None]     # kernels that last read staging buffer 0 / 1
+        buf = 0
+        for w, (segs, needs_stage) in enumerate(waves):
+            if w >= self.max_waves:
+                raise RuntimeError("more waves than the executor's slot arrays hold")
+            for c in cols_needed:
+                self.col_h[w, c, segs] = torch.from_numpy(idx[c][segs])
+            if needs_stage:
+                if done_ev[buf] is not None:
+                    cs.wait_event(done_ev[buf])
+                for j, s in enumerate(segs):
+                    for c in cols_needed:
+                        if idx[c][s] >= 0:
+                            continue
+                        slot = self.stage0 + (buf * self.stage_segments + j) * len(FACT) + c
+                        self.cache.stage(slot, self.host_ptrs[c] + int(s) * SEG * 4, int(self.t.seg_rows[s]),
+                                         cs.cuda_stream)
+                        self.col_h[w, c, s] = slot
+                        staged += 1
+                copied = torch.cuda.Event()
+                copied.record(cs)
+                ks.wait_event(copied)
+            self.seg_h[w, : len(segs)] = torch.from_numpy(segs.astype(np.int16))
+            with torch.cuda.stream(ks):
+                self.col_d[w].copy_(self.col_h[w], non_blocking=True)
+                self.seg_d[w, : len(segs)].copy_(self.seg_h[w, : len(segs)], non_blocking=True)
+            launches += self._launch(w, segs, qarrs, cols_needed, ks)
+            if needs_stage:
+                ev = torch.cuda.Event()
+                ev.record(ks)
+                done_ev[buf] = ev
+                buf ^= 1
+        return launches, len(waves), staged
+
+    # ---- one window ---------------------------------------------------------------------------
+    def run_window(self, queries: list[B.Query], planner) -> WindowRun:
+        t0 = time.perf_counter()
+        ks = self.kstream
+        cands = [self.candidates(q) for q in queries]
+        (preds, saving) = self._predict(planner, queries, cands)
+        copied = self._admit(queries, cands, saving, ks) if saving is not None else 0
+        # per segment: the queries that need it, their CPU ms (with build shares), the batch's GPU ms
+        need: dict[int, list] = {}
+        for qi, (cand, (pc, pg, fc, fg)) in enumerate(zip(cands, preds)):
+            for j, s in enumerate(cand):
+                need.setdefault(int(s), []).append((qi, pc[j] + fc / len(cand), pg[j]))
+        segs = np.array(sorted(need), np.int64)
+        if len(segs):
+            cpu_cost = np.array([sum(x[1] for x in need[s]) for s in segs])
+            gpu_cost = np.array([max(x[2] for x in need[s]) for s in segs])
+            on_gpu, span = place(cpu_cost, gpu_cost)
+        else:
+            on_gpu, span = np.zeros(0, bool), 0.0
+        gsegs, csegs = segs[on_gpu], segs[~on_gpu]
+        plan_ms = (time.perf_counter() - t0) * 1e3
+
+        # result buffers and launch descriptors (chunks of up to 256 queries)
+        flat, views = B.result_buffers(queries)
+        qarrs = []
+        for base in range(0, len(queries), L.MB_BATCH_MAX_QUERIES):
+            chunk = list(range(base, min(len(queries), base + L.MB_BATCH_MAX_QUERIES)))
+            arr = (L.MbBatchQuery * len(chunk))(*[queries[i].to_c(views[i]) for i in chunk])
+            cols = sorted({COL_ID[c] for i in chunk for c in NEEDED[queries[i].template]})
+            qarrs.append((arr, len(chunk), cols))
+        cols_needed = sorted({c for _, _, cols in qarrs for c in cols})
+
+        # CPU share on its own thread: per query, its host tables and its CPU segments
+        host_res = [np.zeros(2 if q.template == "agg" else 4 * q.groups, np.int32) for q in queries]
+        cseg_set = set(int(s) for s in csegs)
+        cpu_ms = [0.0]
+
+        def cpu_share():
+            c0 = time.perf_counter()
+            for qi, (q, cand) in enumerate(zip(queries, cands)):
+                mine = [int(s) for s in cand if int(s) in cseg_set]
+                if mine:
+                    self.build_cpu(q)
+                    self._cpu_segments(q, mine, host_res[qi])
+            cpu_ms[0] = (time.perf_counter() - c0) * 1e3
+
+        th = threading.Thread(target=cpu_share) if len(csegs) else None
+        if th:
+            th.start()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(ks)
+        launches, waves, staged = self._gpu_share(gsegs, qarrs, cols_needed)
+        g1.record(ks)
+        host = torch.empty(flat.numel(), dtype=torch.uint8, pin_memory=True)
+        with torch.cuda.stream(ks):
+            host.copy_(flat, non_blocking=True)
+        if th:
+            th.join()
+        ks.synchronize()
+        hb = host.numpy()
+        results, off = [], 0
+        for q, hr in zip(queries, host_res):
+            nb = 8 if q.template == "agg" else 16 * q.groups
+            g = hb[off: off + nb].view(np.int32).copy()
+            off += nb
+            results.append(merge(q, g, hr) if len(csegs) else g)
+        ms = (time.perf_counter() - t0) * 1e3
+        return WindowRun(results, ms, len(queries), len(segs), len(gsegs), len(csegs), staged, launches, span,
+                         plan_ms=plan_ms, gpu_ms=g0.elapsed_time(g1), cpu_ms=cpu_ms[0], copied_column_segments=copied,
+                         extra={"waves": waves})
+
+    def run(self, queries: list[B.Query], planner, window: int = 256) -> list[WindowRun]:
+        """All queries in windows of `window`, in order."""
+        return [self.run_window(queries[i: i + window], planner) for i in range(0, len(queries), window)]

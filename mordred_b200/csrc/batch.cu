@@ -109,7 +109,10 @@ struct BatchPlan {
   int smem_acc_off, smem_aq_off, smem_res_off, smem_pres_off, smem_out_off, smem_list_off;
   int smem_groups_off, smem_groups_words, smem_stage_off;
   unsigned int* status;
-  const int* fact_all[MB_NUM_FACT_COLS];
+  // segment-cache addressing: col[c] is a per-segment slot array into gpu_cache
+  const int* gpu_cache;
+  const short* seg_group;
+  int seg_shift;
   BQ q[MB_BATCH_MAX_QUERIES];
 };
 static_assert(sizeof(BatchPlan) < 32000, "launch parameter limit");
@@ -126,6 +129,15 @@ __device__ __forceinline__ int field_value(int v, int code) {
   const unsigned shift = (code >> 6) & 31;
   const unsigned mask = width >= 32 ? 0xffffffffu : (1u << width) - 1u;
   return static_cast<int>((static_cast<unsigned>(v) >> shift) & mask);
+}
+
+// Stage column c, row r, read from global memory (direct, or through the segment cache).
+__device__ __forceinline__ int batch_load(const BatchPlan& P, int c, long long r) {
+  if (P.gpu_cache == nullptr) return __ldg(P.col[c] + r);
+  const long long vseg = r >> P.seg_shift;
+  const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg]) : static_cast<int>(vseg);
+  return __ldg(P.gpu_cache + (static_cast<long long>(__ldg(P.col[c] + seg)) << P.seg_shift) +
+               (r & ((1ll << P.seg_shift) - 1)));
 }
 
 __device__ __forceinline__ void bmbar_arrive(uint64_t* bar) {
@@ -329,7 +341,24 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         int* dst = stage_base + s * P.stage_words;
         fence_proxy_async_smem();
         mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>(P.ncols) * TILE * 4u);
-        for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * CS, P.col[c] + r0, TILE * 4, &full[s], policy);
+        if (P.gpu_cache == nullptr) {
+          for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * CS, P.col[c] + r0, TILE * 4, &full[s], policy);
+        } else {
+          // through the segment cache: a tile that crosses a segment boundary is copied in
+          // two pieces (row offsets are multiples of 4, so every piece is 16-byte aligned)
+          const long long S = 1ll << P.seg_shift;
+          for (int done = 0; done < TILE;) {
+            const long long r = r0 + done;
+            const long long vseg = r >> P.seg_shift;
+            const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg]) : static_cast<int>(vseg);
+            const long long in = r & (S - 1);
+            const int take = static_cast<int>(S - in < TILE - done ? S - in : TILE - done);
+            for (int c = 0; c < P.ncols; ++c)
+              bulk_g2s(dst + c * CS + done, P.gpu_cache + (static_cast<long long>(P.col[c][seg]) << P.seg_shift) + in,
+                       static_cast<uint32_t>(take) * 4u, &full[s], policy);
+            done += take;
+          }
+        }
         if (++s == S) {
           s = 0;
           phase ^= 1u;
@@ -475,7 +504,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         uint32_t pr = 0;
         for (int t = 0; t < P.ndims; ++t) {
           const int d = P.dim_list[t];
-          const int h = bslot(__ldg(P.col[P.key_stage[d]] + r), P.pat_slots[d], P.pat_kmin[d]);
+          const int h = bslot(batch_load(P, P.key_stage[d], r), P.pat_slots[d], P.pat_kmin[d]);
           if (h < 0) {
             bad_probe = true;
             continue;
@@ -486,7 +515,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
         auto get = [&](int code) {
           const int c = code >> 11;
           const int d = P.stage_dim[c];
-          return field_value(d >= 0 ? dimw[d] : __ldg(P.col[c] + r), code);
+          return field_value(d >= 0 ? dimw[d] : batch_load(P, c, r), code);
         };
         unsigned m[NWM];
         batch_row_mask<NWM>(P, pr, get, s_pres, s_out, smem, m);
@@ -762,10 +791,19 @@ static int plan_batch(const mb_batch_args* a, BatchPlan& P) {
   }
   for (int c = 0; c < 13; ++c) P.cidx[c] = -1;
   for (int c = 0; c < kMaxStageCols; ++c) P.stage_dim[c] = -1;
+  if (a->gpu_cache != nullptr) {
+    const int ss = a->segment_size;
+    if (ss < 4 || (ss & (ss - 1)) != 0) return MB_ERR_ARG;
+    if (!aligned16(a->gpu_cache)) return MB_ERR_ALIGN;
+    P.gpu_cache = a->gpu_cache;
+    P.seg_group = a->segment_group;
+    P.seg_shift = __builtin_ctz(static_cast<unsigned>(ss));
+  } else if (a->segment_group != nullptr) {
+    return MB_ERR_ARG;
+  }
   for (int c = 0; c < MB_NUM_FACT_COLS; ++c) {
-    P.fact_all[c] = a->fact[c];
     if (!fact_used[c]) continue;
-    if (!aligned16(a->fact[c])) return MB_ERR_ALIGN;
+    if (P.gpu_cache == nullptr && !aligned16(a->fact[c])) return MB_ERR_ALIGN;
     P.cidx[c] = P.ncols;
     P.col[P.ncols++] = a->fact[c];
   }

@@ -39,6 +39,7 @@ struct mb_segcache {
   std::vector<uint64_t> uses;
   std::vector<double> weight;
   std::vector<int> free_slots;
+  int64_t reserved = 0;            // the top `reserved` slots are the caller's (staging)
   uint64_t stamp = 1;
   mb_segcache_stats stats{};
   std::mutex mu;
@@ -258,7 +259,7 @@ extern "C" int mb_segcache_replace(mb_segcache* c, const double* weights, const 
   for (size_t k = 0; k < keys; ++k)
     if (weights[k] > 0) order.push_back(static_cast<int>(k));
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return weights[x] > weights[y]; });
-  if (static_cast<int64_t>(order.size()) > c->num_slots) order.resize(c->num_slots);
+  if (static_cast<int64_t>(order.size()) > c->num_slots - c->reserved) order.resize(c->num_slots - c->reserved);
   std::vector<char> keep(keys, 0);
   for (int k : order) keep[k] = 1;
   for (int64_t s = 0; s < c->num_slots; ++s)
@@ -284,6 +285,36 @@ extern "C" int mb_segcache_get_stats(mb_segcache* c, mb_segcache_stats* out) {
   if (c == nullptr || out == nullptr) return MB_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   *out = c->stats;
-  out->resident = static_cast<unsigned long long>(c->num_slots - static_cast<int64_t>(c->free_slots.size()));
+  out->resident =
+      static_cast<unsigned long long>(c->num_slots - c->reserved - static_cast<int64_t>(c->free_slots.size()));
   return MB_OK;
+}
+
+extern "C" int mb_segcache_reserve(mb_segcache* c, int64_t nslots, int64_t* first_slot) {
+  if (c == nullptr || nslots < 0 || first_slot == nullptr) return MB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (nslots >= c->num_slots - c->reserved) return MB_ERR_SIZE;
+  const int64_t lo = c->num_slots - c->reserved - nslots, hi = c->num_slots - c->reserved;
+  for (int64_t s = lo; s < hi; ++s)
+    if (c->owner[s] >= 0) release(c, static_cast<int>(s));
+  // take [lo, hi) out of the free list and out of every policy's reach
+  std::vector<int> keep;
+  keep.reserve(c->free_slots.size());
+  for (int s : c->free_slots)
+    if (s < lo || s >= hi) keep.push_back(s);
+  c->free_slots.swap(keep);
+  for (int64_t s = lo; s < hi; ++s) c->owner[s] = -2;
+  c->reserved += nslots;
+  *first_slot = lo;
+  return MB_OK;
+}
+
+extern "C" int mb_segcache_stage(mb_segcache* c, int64_t slot, const int* host_src, int rows, mb_stream_t stream) {
+  if (c == nullptr || host_src == nullptr || rows < 0 || rows > c->segment_size) return MB_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (slot < c->num_slots - c->reserved || slot >= c->num_slots) return MB_ERR_ARG;  // reserved slots only
+    c->stats.bytes_h2d += static_cast<unsigned long long>(rows) * 4;
+  }
+  return copy_in(c, static_cast<int>(slot), host_src, rows, static_cast<cudaStream_t>(stream));
 }

@@ -139,28 +139,23 @@ class QueryRun:
     extra: dict = field(default_factory=dict)
 
 
-class Executor:
-    def __init__(self, table: SegmentedTable, cache_slots: int = 2048, policy: str = "lru", device: int = 0,
-                 max_waves: int = 16):
-        self.t = table
-        self.cache = SegmentCache(cache_slots, SEG, len(FACT), table.nseg, policy, device)
-        s = table.sizes
-        z = lambda n: torch.zeros(n, dtype=torch.int32, device="cuda")
-        self.ht = {"s": z(s.s_len), "c": z(2 * s.c_len), "p_key": z(s.p_len), "p_kv": z(2 * s.p_len),
-                   "d": z(2 * ssb.DATE_SLOTS)}
-        self.hht = {k: np.zeros(v.numel(), np.int32) for k, v in self.ht.items()}
-        self.max_waves = max_waves
-        self.col_idx_h = torch.empty(max_waves, len(FACT), table.nseg, dtype=torch.int32, pin_memory=True)
-        self.col_idx_d = torch.empty(max_waves, len(FACT), table.nseg, dtype=torch.int32, device="cuda")
-        self.seg_h = torch.empty(max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
-        self.seg_d = torch.empty(max_waves, table.nseg, dtype=torch.int16, device="cuda")
-        self.res_d = torch.zeros(4 * ssb.QA_GROUPS, dtype=torch.int32, device="cuda")
-        self.res_h = torch.empty(4 * ssb.QA_GROUPS, dtype=torch.int32, pin_memory=True)
-        self.cpu_threads = cpu.threads()
-        self._host_ptrs = [table.ptr(c, 0) if c in table.host else None for c in FACT]
-        self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+def host_tables(sizes: ssb.Sizes) -> dict:
+    """Zeroed host hash tables of the three query forms (the CPU share's builds)."""
+    n = {"s": sizes.s_len, "c": 2 * sizes.c_len, "p_key": sizes.p_len, "p_kv": 2 * sizes.p_len,
+         "d": 2 * ssb.DATE_SLOTS}
+    return {k: np.zeros(v, np.int32) for k, v in n.items()}
 
-    # ---- planning inputs ----------------------------------------------------------------
+
+class CpuShare:
+    """Segment skipping, the fused pipeline's arguments and the CPU side of a query's
+    segments: filtered builds of its hash tables on the host (build_CPU,
+    CPUProcessing.cu:1034-1104) and the fused pipeline over a list of segments of the
+    pinned host columns (CPUProcessing.cu:723-866). Needs `t` (the table) and `hht` (host
+    hash tables, :func:`host_tables`)."""
+
+    t: SegmentedTable
+    hht: dict
+
     def candidates(self, q: B.Query) -> np.ndarray:
         """Segments whose orderdate [min, max] meets the query's range (and, for the
         filter-aggregate, whose discount and quantity ranges meet the query's)."""
@@ -171,53 +166,6 @@ class Executor:
                 if name in t.min:
                     ok &= (t.max[name] >= r[0]) & (t.min[name] <= r[1])
         return np.nonzero(ok)[0]
-
-    def context(self, q: B.Query, segs: np.ndarray) -> QueryContext:
-        """The planners' view of q over `segs`: rows, in-range share of each segment's
-        rows (the table is date-sorted, so a segment's dates are contiguous), residency of
-        the needed columns, hash-table sizes."""
-        t = self.t
-        segs = np.asarray(segs, np.int64)
-        lo, hi = t.seg_day_lo[segs], t.seg_day_hi[segs]
-        qlo, qhi = _day(q.date[0]), _day(q.date[1] + 1) - 1
-        inter = np.maximum(0, np.minimum(hi, qhi) - np.maximum(lo, qlo) + 1)
-        date_sel = inter / np.maximum(1, hi - lo + 1)
-        need = NEEDED[q.template]
-        res = np.zeros(len(segs), np.int32)
-        for c in need:
-            res += self.cache.col_idx(COL_ID[c])[segs] >= 0
-        s = t.sizes
-        ht_bytes = {"agg": 0, "qa": 4 * (s.s_len + 2 * s.p_len + 2 * ssb.DATE_SLOTS),
-                    "qb": 4 * (s.s_len + 2 * s.c_len + s.p_len + 2 * ssb.DATE_SLOTS)}[q.template]
-        dim_rows = {"agg": 0, "qa": s.s_len + s.p_len + s.d_len, "qb": s.s_len + s.c_len + s.p_len + s.d_len}
-        free = 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
-        return QueryContext(q.template, t.seg_rows[segs].astype(np.float64), date_sel.astype(np.float64),
-                            _small_sel(q), len(need), res, ht_bytes, dim_rows[q.template], q.groups,
-                            self.cpu_threads, free)
-
-    # ---- builds ------------------------------------------------------------------------
-    def build_gpu(self, q: B.Query) -> None:
-        if q.template == "agg":
-            return
-        d, s, st = self.t.dims, self.t.sizes, ssb._stream()
-        BT = L.MB_FILTER_BETWEEN
-        self.ht["s"].zero_()
-        self.ht["d"].zero_()
-        L.call("mb_build_pht", ssb._p(d["s_region"]), BT, q.s_region[0], q.s_region[1], ssb._p(d["s_suppkey"]), None,
-               s.s_len, ssb._p(self.ht["s"]), s.s_len, 0, None, st)
-        L.call("mb_build_pht", None, 0, 0, 0, ssb._p(d["d_datekey"]), ssb._p(d["d_year"]), s.d_len,
-               ssb._p(self.ht["d"]), ssb.DATE_SLOTS, ssb.DATE_MIN, None, st)
-        if q.template == "qa":
-            self.ht["p_kv"].zero_()
-            L.call("mb_build_pht", ssb._p(d["p_category"]), BT, q.category[0], q.category[1], ssb._p(d["p_partkey"]),
-                   ssb._p(d["p_brand1"]), s.p_len, ssb._p(self.ht["p_kv"]), s.p_len, 0, None, st)
-        else:
-            self.ht["c"].zero_()
-            self.ht["p_key"].zero_()
-            L.call("mb_build_pht", ssb._p(d["c_region"]), BT, q.c_region[0], q.c_region[1], ssb._p(d["c_custkey"]),
-                   ssb._p(d["c_nation"]), s.c_len, ssb._p(self.ht["c"]), s.c_len, 0, None, st)
-            L.call("mb_build_pht", ssb._p(d["p_mfgr"]), BT, q.mfgr[0], q.mfgr[1], ssb._p(d["p_partkey"]), None,
-                   s.p_len, ssb._p(self.ht["p_key"]), s.p_len, 0, None, st)
 
     def build_cpu(self, q: B.Query) -> None:
         if q.template == "agg":
@@ -242,7 +190,6 @@ class Executor:
             cpu.build_pht(d["p_mfgr"], BT, q.mfgr[0], q.mfgr[1], d["p_partkey"], None, h["p_key"], s.p_len, 0,
                           L.MB_HT_KEY)
 
-    # ---- the fused pipeline's arguments --------------------------------------------------
     def args(self, q: B.Query, col, ht: dict, n_rows: int, res, **extra) -> L.MbStarArgs:
         """mb_star_args of query q; col(name) gives a column (pointer or array), ht the tables."""
         s = self.t.sizes
@@ -281,6 +228,82 @@ class Executor:
 
     def _rows(self, segs: np.ndarray) -> int:
         return int(self.t.seg_rows[segs].sum())
+
+    def _cpu_segments(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
+        segs = self._order(np.array(csegs), self.t)
+        group = segs.astype(np.int16)  # the arguments hold its address: keep it alive through the call
+        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res, segment_group=group,
+                      segment_size=SEG)
+        cpu.star_query(a)
+
+    def context(self, q: B.Query, segs: np.ndarray) -> QueryContext:
+        """The planners' view of q over `segs`: rows, in-range share of each segment's
+        rows (the table is date-sorted, so a segment's dates are contiguous), residency of
+        the needed columns, hash-table sizes. Needs `cache` and `cpu_threads` too."""
+        t = self.t
+        segs = np.asarray(segs, np.int64)
+        lo, hi = t.seg_day_lo[segs], t.seg_day_hi[segs]
+        qlo, qhi = _day(q.date[0]), _day(q.date[1] + 1) - 1
+        inter = np.maximum(0, np.minimum(hi, qhi) - np.maximum(lo, qlo) + 1)
+        date_sel = inter / np.maximum(1, hi - lo + 1)
+        need = NEEDED[q.template]
+        res = np.zeros(len(segs), np.int32)
+        for c in need:
+            res += self.cache.col_idx(COL_ID[c])[segs] >= 0
+        s = t.sizes
+        ht_bytes = {"agg": 0, "qa": 4 * (s.s_len + 2 * s.p_len + 2 * ssb.DATE_SLOTS),
+                    "qb": 4 * (s.s_len + 2 * s.c_len + s.p_len + 2 * ssb.DATE_SLOTS)}[q.template]
+        dim_rows = {"agg": 0, "qa": s.s_len + s.p_len + s.d_len, "qb": s.s_len + s.c_len + s.p_len + s.d_len}
+        free = 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
+        return QueryContext(q.template, t.seg_rows[segs].astype(np.float64), date_sel.astype(np.float64),
+                            _small_sel(q), len(need), res, ht_bytes, dim_rows[q.template], q.groups,
+                            self.cpu_threads, free)
+
+
+class Executor(CpuShare):
+    def __init__(self, table: SegmentedTable, cache_slots: int = 2048, policy: str = "lru", device: int = 0,
+                 max_waves: int = 16):
+        self.t = table
+        self.cache = SegmentCache(cache_slots, SEG, len(FACT), table.nseg, policy, device)
+        s = table.sizes
+        z = lambda n: torch.zeros(n, dtype=torch.int32, device="cuda")
+        self.ht = {"s": z(s.s_len), "c": z(2 * s.c_len), "p_key": z(s.p_len), "p_kv": z(2 * s.p_len),
+                   "d": z(2 * ssb.DATE_SLOTS)}
+        self.hht = host_tables(s)
+        self.max_waves = max_waves
+        self.col_idx_h = torch.empty(max_waves, len(FACT), table.nseg, dtype=torch.int32, pin_memory=True)
+        self.col_idx_d = torch.empty(max_waves, len(FACT), table.nseg, dtype=torch.int32, device="cuda")
+        self.seg_h = torch.empty(max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
+        self.seg_d = torch.empty(max_waves, table.nseg, dtype=torch.int16, device="cuda")
+        self.res_d = torch.zeros(4 * ssb.QA_GROUPS, dtype=torch.int32, device="cuda")
+        self.res_h = torch.empty(4 * ssb.QA_GROUPS, dtype=torch.int32, pin_memory=True)
+        self.cpu_threads = cpu.threads()
+        self._host_ptrs = [table.ptr(c, 0) if c in table.host else None for c in FACT]
+        self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    # ---- builds ------------------------------------------------------------------------
+    def build_gpu(self, q: B.Query) -> None:
+        if q.template == "agg":
+            return
+        d, s, st = self.t.dims, self.t.sizes, ssb._stream()
+        BT = L.MB_FILTER_BETWEEN
+        self.ht["s"].zero_()
+        self.ht["d"].zero_()
+        L.call("mb_build_pht", ssb._p(d["s_region"]), BT, q.s_region[0], q.s_region[1], ssb._p(d["s_suppkey"]), None,
+               s.s_len, ssb._p(self.ht["s"]), s.s_len, 0, None, st)
+        L.call("mb_build_pht", None, 0, 0, 0, ssb._p(d["d_datekey"]), ssb._p(d["d_year"]), s.d_len,
+               ssb._p(self.ht["d"]), ssb.DATE_SLOTS, ssb.DATE_MIN, None, st)
+        if q.template == "qa":
+            self.ht["p_kv"].zero_()
+            L.call("mb_build_pht", ssb._p(d["p_category"]), BT, q.category[0], q.category[1], ssb._p(d["p_partkey"]),
+                   ssb._p(d["p_brand1"]), s.p_len, ssb._p(self.ht["p_kv"]), s.p_len, 0, None, st)
+        else:
+            self.ht["c"].zero_()
+            self.ht["p_key"].zero_()
+            L.call("mb_build_pht", ssb._p(d["c_region"]), BT, q.c_region[0], q.c_region[1], ssb._p(d["c_custkey"]),
+                   ssb._p(d["c_nation"]), s.c_len, ssb._p(self.ht["c"]), s.c_len, 0, None, st)
+            L.call("mb_build_pht", ssb._p(d["p_mfgr"]), BT, q.mfgr[0], q.mfgr[1], ssb._p(d["p_partkey"]), None,
+                   s.p_len, ssb._p(self.ht["p_key"]), s.p_len, 0, None, st)
 
     def _launch_wave(self, q: B.Query, segs: list[int], w: int) -> None:
         segs = self._order(np.array(segs), self.t)
@@ -453,14 +476,6 @@ class Executor:
                         "resident_frac": float(ctx.resident_cols[i]) / ctx.needed_cols})
         return out, {"template": q.template, "cpu_build_ms": cpu_build, "gpu_build_ms": gpu_build,
                      "segments": len(okseg), "gpu_batch_kernel_ms": kbatch, "cpu_batch_ms": cbatch}
-
-    def _cpu_segments(self, q: B.Query, csegs: list[int], res: np.ndarray) -> None:
-        segs = self._order(np.array(csegs), self.t)
-        group = segs.astype(np.int16)  # the arguments hold its address: keep it alive through the call
-        a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res, segment_group=group,
-                      segment_size=SEG)
-        cpu.star_query(a)
-
 
 def merge(q: B.Query, gpu: np.ndarray, cpu_res: np.ndarray) -> np.ndarray:
     """Add the CPU share's result into the GPU share's (src/gpudb/CPUProcessing.cu:

@@ -149,6 +149,9 @@ class AnalyticPlanner:
         cpu, gpu = analytic_ms(ctx)
         return cpu, gpu, float(L.lib().mb_cost_build_ms(float(ctx.dim_rows))), 0.0
 
+    def predict_many(self, ctxs: list[QueryContext]) -> list:
+        return [self.predict(c) for c in ctxs]
+
 
 class LearnedPlanner:
     """The cost MLP on the GPU. `params` is the flat fp32 parameter vector (5,890)."""
@@ -182,6 +185,18 @@ class LearnedPlanner:
             return np.zeros(0), np.zeros(0), fc, fg
         y = np.exp(self.predict_log(features(ctx)))
         return y[:, 0], y[:, 1], fc, fg
+
+    def predict_many(self, ctxs: list[QueryContext]) -> list:
+        """predict() for many queries with one model call over all their segments."""
+        feats = [features(c) for c in ctxs if len(c)]
+        y = np.exp(self.predict_log(np.concatenate(feats))) if feats else np.zeros((0, 2))
+        out, off = [], 0
+        for c in ctxs:
+            fc, fg = self.fixed_ms.get(c.template, [0.0, 0.0])
+            n = len(c)
+            out.append((y[off: off + n, 0], y[off: off + n, 1], fc, fg))
+            off += n
+        return out
 
     def train(self, feats: np.ndarray, log_ms: np.ndarray, epochs: int = 40, batch: int = 256, lr: float = 2e-3,
               weight_decay: float = 1e-5, seed: int = 0) -> dict:

@@ -105,7 +105,17 @@ def mae_report(pred: np.ndarray, truth: np.ndarray) -> dict:
             "mae_log_ms": float(err.mean())}
 
 
-def evaluate(ex: Executor, planners: list, queries: list[B.Query], start_weights: np.ndarray, log=print) -> dict:
+def completion_stats(ms: list[float]) -> dict:
+    """Latency of queries that all arrived at time 0 and ran in the given order: each one's
+    completion time is the running total of the service times before and including it."""
+    done = np.cumsum(ms)
+    return {"p50_completion_ms": float(np.percentile(done, 50)), "p99_completion_ms": float(np.percentile(done, 99))}
+
+
+def evaluate(ex: Executor, planners: list, queries: list[B.Query], start_weights: np.ndarray, log=print,
+             keep_results: dict | None = None) -> dict:
+    """Run `queries` one at a time under each planner from the same starting cache. When
+    keep_results is a dict, each planner's per-query results are stored in it by name."""
     out = {}
     results = {}
     for p in planners:
@@ -130,16 +140,55 @@ def evaluate(ex: Executor, planners: list, queries: list[B.Query], start_weights
             for k in ("pred_gpu_ms", "pred_cpu_ms", "plan_ms"):
                 diag[k] += r.extra.get(k, 0.0)
         results[p.name] = res
+        if keep_results is not None:
+            keep_results[p.name] = res
         ms_sorted = sorted(ms)
         out[p.name] = {"total_ms": float(sum(ms)), "mean_ms": float(statistics.mean(ms)),
                        "p50_ms": float(ms_sorted[len(ms) // 2]),
                        "p99_ms": float(ms_sorted[min(len(ms) - 1, int(math.ceil(0.99 * len(ms))) - 1)]),
+                       **completion_stats(ms),
                        "gpu_segments": gseg, "cpu_segments": cseg, "column_segments_admitted": adm,
                        "sums": diag}
         log(f"  {p.name}: total {out[p.name]['total_ms']:.0f} ms over {len(queries)} queries, "
             f"p50 {out[p.name]['p50_ms']:.2f}, p99 {out[p.name]['p99_ms']:.2f}, gpu/cpu segments {gseg}/{cseg}")
     names = list(results)
     out["results_identical"] = all(np.array_equal(a, b) for a, b in zip(results[names[0]], results[names[-1]]))
+    return out
+
+
+def evaluate_batched(bx, planners: list, queries: list[B.Query], start_weights: np.ndarray, window: int = 256,
+                     log=print, keep_results: dict | None = None) -> dict:
+    """Run `queries` in windows of `window` through the batched executor under each planner,
+    from the same starting cache (and no carried-over benefit weights)."""
+    out = {}
+    for p in planners:
+        bx.benefit[:] = 0.0
+        bx.cache.replace(start_weights, bx.host_ptrs, bx.t.seg_rows)
+        bx.run_window(queries[:8], p)           # loads kernels, pool threads, model
+        bx.benefit[:] = 0.0
+        bx.cache.replace(start_weights, bx.host_ptrs, bx.t.seg_rows)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        runs = bx.run(queries, p, window=window)
+        total = (time.perf_counter() - t0) * 1e3
+        res = [r for w in runs for r in w.results]
+        if keep_results is not None:
+            keep_results[p.name] = res
+        done = np.cumsum([w.ms for w in runs])
+        per_query = np.repeat(done, [w.queries for w in runs])
+        out[p.name] = {"total_ms": total, "windows": len(runs), "window_queries": window,
+                       "mean_window_ms": float(np.mean([w.ms for w in runs])),
+                       "p50_completion_ms": float(np.percentile(per_query, 50)),
+                       "p99_completion_ms": float(np.percentile(per_query, 99)),
+                       "union_segments": int(sum(w.union_segments for w in runs)),
+                       "gpu_segments": int(sum(w.gpu_segments for w in runs)),
+                       "cpu_segments": int(sum(w.cpu_segments for w in runs)),
+                       "staged_column_segments": int(sum(w.staged_segments for w in runs)),
+                       "admitted_column_segments": int(sum(w.copied_column_segments for w in runs)),
+                       "launches": int(sum(w.launches for w in runs)),
+                       "plan_ms": float(sum(w.plan_ms for w in runs)), "gpu_ms": float(sum(w.gpu_ms for w in runs)),
+                       "cpu_ms": float(sum(w.cpu_ms for w in runs))}
+        log(f"  batched {p.name}: total {total:.0f} ms over {len(queries)} queries in {len(runs)} windows")
     return out
 
 

@@ -85,6 +85,17 @@ class SegmentCache:
         rows = np.ascontiguousarray(segment_rows, dtype=np.int32)
         L.call("mb_segcache_replace", self.h, w.ctypes.data, ptrs, rows.ctypes.data, stream)
 
+    def reserve(self, nslots: int) -> int:
+        """Take the top `nslots` unreserved slots out of management (a staging area the
+        caller copies into); returns the first reserved slot."""
+        first = C.c_int64(0)
+        L.call("mb_segcache_reserve", self.h, nslots, C.byref(first))
+        return int(first.value)
+
+    def stage(self, slot: int, host_ptr: int, rows: int, stream: int = 0) -> None:
+        """Copy a segment's rows into reserved slot `slot` (asynchronous on `stream`)."""
+        L.call("mb_segcache_stage", self.h, slot, host_ptr, rows, stream)
+
     def stats(self) -> dict:
         s = L.MbSegcacheStats()
         L.call("mb_segcache_get_stats", self.h, C.byref(s))

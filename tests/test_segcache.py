@@ -99,3 +99,36 @@ def test_admit_segments_in_order_until_full():
     c.begin_query()
     done, copied = c.admit_segments([0, 2], [5, 0], [x.ctypes.data for x in cols], rows)
     assert done == 2 and copied == 1  # segment 5 resident; segment 0's first column was copied before
+
+
+def test_reserved_staging_slots_are_never_used_by_the_cache():
+    cols = _cols(1, 10)
+    c = SegmentCache(6, SEG, 1, 10, "lru", device=-1)
+    c.begin_query()
+    for seg in range(6):
+        c.admit(0, seg, cols[0][seg * SEG:].ctypes.data, SEG)
+    first = c.reserve(2)               # evicts what the top two slots held
+    assert first == 4
+    assert c.stats()["resident"] == 4
+    assert all(s < 4 for s in c.col_idx(0) if s >= 0)
+    # admissions and epoch replacement stay within the four managed slots
+    for seg in range(6, 10):
+        c.begin_query()
+        assert c.admit(0, seg, cols[0][seg * SEG:].ctypes.data, SEG) < 4
+    w = np.arange(10, dtype=np.float64)[None, :] + 1.0
+    c.replace(w, [cols[0].ctypes.data], np.full(10, SEG, np.int32))
+    idx = c.col_idx(0)
+    assert sorted(np.nonzero(idx >= 0)[0].tolist()) == [6, 7, 8, 9] and all(s < 4 for s in idx if s >= 0)
+    with pytest.raises(L.MbError):
+        c.reserve(4)                   # would leave no managed slot
+
+
+def test_stage_copies_into_reserved_slots_only():
+    cols = _cols(1, 4)
+    c = SegmentCache(5, SEG, 1, 4, "lru", device=-1)
+    first = c.reserve(2)
+    c.stage(first + 1, cols[0][2 * SEG:].ctypes.data, SEG)
+    assert np.array_equal(c.host_slot_view(first + 1), cols[0][2 * SEG: 3 * SEG])
+    assert (c.col_idx(0) == -1).all()           # staging leaves the map alone
+    with pytest.raises(L.MbError):
+        c.stage(0, cols[0].ctypes.data, SEG)     # a managed slot
