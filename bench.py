@@ -333,7 +333,7 @@ def batch_section(t, s, n, rank, world, args):
             "launch": "CUDA graph replay (result memset + mask kernel + batch kernel)", "seed": SEED}
 
 
-def planner_section(args):
+def planner_section(args, table=None):
     """Config 3: a host-resident, date-sorted fact table of --planner-rows rows (1 Mi-row
     segments, per-segment min/max) under an 8 GB GPU segment-cache budget, and
     --planner-queries generated queries. The plain form runs them one at a time (the
@@ -356,7 +356,8 @@ def planner_section(args):
         return {"unavailable": "no trained planner weights in mordred_b200/planner_weights"}
     learned = LearnedPlanner.load(PE.DEFAULT_WEIGHTS)
     t0 = time.perf_counter()
-    table = SegmentedTable(args.planner_rows, SEED)
+    if table is None:
+        table = SegmentedTable(args.planner_rows, SEED)
     slots = int(8 * (1 << 30) // (SEG * 4))
     setup_s = time.perf_counter() - t0
     queries = B.generate_queries(args.planner_queries, seed=SEED + 7)
@@ -408,36 +409,82 @@ def planner_section(args):
             "weights": "mordred_b200/planner_weights/mlp.bin", "seed": SEED}
 
 
-def serve_section(args):
-    """The serving loop: Poisson arrivals at --serve-rate over a GPU-resident table of
-    --serve-rows rows, a 16 GB admission budget, the batched kernel (up to 256 queries a
-    launch). The reported server runs whole-scan batches; the same arrivals through the
-    circular scan (admitted queries join the running scan at the next of 8 chunks and
-    complete after one lap) are reported beside it. Latency: arrival to completion."""
+def serve_section(args, table=None):
+    """Config 5, the serving loop: Poisson arrivals at --serve-rate over a GPU-resident,
+    date-sorted table of --serve-rows rows, a 16 GB admission budget, the batched kernel.
+    Two GPU servers — whole-scan batches (up to 256 queries a launch) and the circular scan
+    (admitted queries join the running scan at the next of 8 chunks and complete after one
+    lap, at most 128 at a time) — each with the learned planner routing the queries it
+    predicts the host cores answer sooner to the CPU engine; over three arrival seeds, and
+    once without the router for comparison. Latency: arrival to completion. Results are
+    checked against the queries run alone for a sample."""
+    import numpy as np
     import torch
 
     from mordred_b200 import batch as B
+    from mordred_b200 import planner_experiment as PE
     from mordred_b200 import serve as S
     from mordred_b200 import ssb
+    from mordred_b200.engine import SegmentedTable
+    from mordred_b200.planner import LearnedPlanner
 
-    sizes = ssb.Sizes(lo_len=args.serve_rows)
-    t = ssb.gen_device(sizes, SEED, B.BATCH_FACT, B.BATCH_DIMS)
+    if table is None or table.n != args.serve_rows:
+        table = SegmentedTable(args.serve_rows, SEED)
+    sizes = table.sizes
+    t = {k: torch.empty(table.n, dtype=torch.int32, device="cuda") for k in B.BATCH_FACT}
+    for k in B.BATCH_FACT:
+        t[k].copy_(table.host_t[k])
+    t.update(table.dims)
+    t.update(ssb.gen_device(sizes, SEED, [], [d for d in B.BATCH_DIMS if d not in t]))
     n = int(args.serve_rate * args.serve_seconds)
+    planner = LearnedPlanner.load(PE.DEFAULT_WEIGHTS) if os.path.exists(PE.DEFAULT_WEIGHTS) else None
+    whole = S.Server(t, sizes, table.n, 16 << 30)
+    circ = S.CircularServer(t, sizes, table.n, 16 << 30, chunks=8)
+    whole.run_batch(B.generate_queries(8, seed=1))
+    keys = ("qps", "p50_ms", "p90_ms", "p99_ms", "max_ms", "batches", "mean_batch", "mean_batch_ms", "cpu_answered")
+    runs = {"whole": [], "circular": []}
+    routing = []
+    checked = 0
+    for k, seed in enumerate((SEED + 3, SEED + 31, SEED + 57)):
+        qs = B.generate_queries(n, seed=seed)
+        arrivals = S.poisson_arrivals(args.serve_rate, n, seed + 2)
+        for name, srv in (("whole", whole), ("circular", circ)):
+            router = S.PlannerRouter(table, planner) if planner is not None else None
+            rep, res = srv.serve(qs, arrivals, router=router, keep_results=(k == 0))
+            if router is not None:
+                routing.append(router.summary())
+                router.close()
+            summ = rep.summary(table.n)
+            runs[name].append({kk: summ[kk] for kk in keys})
+            if k == 0:
+                ws = B.AloneWorkspace(sizes)
+                for qid in range(0, n, max(1, n // 40)):
+                    r = qs[qid].result_buffer()
+                    B.run_alone(t, ws, qs[qid], r, table.n)
+                    exp = r.cpu().numpy().reshape(-1)
+                    got = np.asarray(res[qid]).reshape(-1)
+                    assert np.array_equal(got.view(exp.dtype), exp), (name, qid)
+                    checked += 1
+    # the same first arrivals without the router: every query on the GPU
     qs = B.generate_queries(n, seed=SEED + 3)
     arrivals = S.poisson_arrivals(args.serve_rate, n, SEED + 5)
-    whole = S.Server(t, sizes, args.serve_rows, 16 << 30)
-    whole.run_batch(qs[:8])
-    rep_w, _ = whole.serve(qs, arrivals)
-    circ = S.CircularServer(t, sizes, args.serve_rows, 16 << 30, chunks=8)
-    rep, _ = circ.serve(qs, arrivals)
-    sc = rep.summary(args.serve_rows)
-    out = dict(rep_w.summary(args.serve_rows), server="whole-scan batches", rows=args.serve_rows,
-               rate_qps=args.serve_rate, budget_bytes=16 << 30, selectivity="log-uniform in [1e-5, 0.3]", seed=SEED,
-               circular_scan_8_chunks={k: sc[k] for k in ("qps", "p50_ms", "p90_ms", "p99_ms", "max_ms", "batches",
-                                                          "mean_batch", "mean_batch_ms")})
+    no_router = {}
+    for name, srv in (("whole", whole), ("circular", circ)):
+        rep, _ = srv.serve(qs, arrivals)
+        summ = rep.summary(table.n)
+        no_router[name] = {kk: summ[kk] for kk in keys}
     del whole, circ, t
     torch.cuda.empty_cache()
-    return out
+    p99 = lambda name: [r["p99_ms"] for r in runs[name]]
+    return {"rows": table.n, "rate_qps": args.serve_rate, "seconds_per_run": args.serve_seconds,
+            "budget_bytes": 16 << 30, "table": "date-sorted, GPU-resident (9 fact columns)",
+            "selectivity": "log-uniform in [1e-5, 0.3]", "seeds": 3, "router": "learned planner" if planner else None,
+            "whole_scan_batches": runs["whole"], "circular_scan_8_chunks_max_128_active": runs["circular"],
+            "p99_ms_whole_by_seed": p99("whole"), "p99_ms_circular_by_seed": p99("circular"),
+            "without_router_first_seed": no_router, "routing": routing,
+            "results_checked_against_alone": checked,
+            "qps": runs["circular"][0]["qps"], "p50_ms": runs["circular"][0]["p50_ms"],
+            "p99_ms": max(p99("circular"))}
 
 
 def summary_of(per_query, batched, planner, serving) -> dict:
@@ -643,17 +690,20 @@ def main():
                "h2d_gbs": runner.h2d_bytes / e_ms / 1e6,
                "bound": "host-to-device copies (PCIe Gen5 x16, 64 GB/s nominal per direction)"}
 
-    # ---- serving loop over a 600 M-row resident table (N = 1) -------------------------------
-    serving = None
+    # ---- config 3 (planner, host-resident table) and config 5 (serving) share one date-sorted
+    # 600 M-row table in pinned host memory (N = 1) --------------------------------------------
+    planner = serving = None
+    table = None
+    if world == 1 and (not args.no_planner or not args.no_serve):
+        from mordred_b200.engine import SegmentedTable
+        torch.cuda.empty_cache()
+        table = SegmentedTable(args.planner_rows, SEED)
+    if world == 1 and not args.no_planner:
+        planner = planner_section(args, table)
     if world == 1 and not args.no_serve:
         torch.cuda.empty_cache()
-        serving = serve_section(args)
-
-    # ---- learned vs analytic planner over a host-resident table (N = 1) --------------------
-    planner = None
-    if world == 1 and not args.no_planner:
-        torch.cuda.empty_cache()
-        planner = planner_section(args)
+        serving = serve_section(args, table)
+    del table
 
     # ---- CPU baseline on the host cores (rank 0, N = 1) -------------------------------------
     cpu = None

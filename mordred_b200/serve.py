@@ -18,13 +18,21 @@ src/gpudb/main.cu:72-489, one at a time). Here:
 * :class:`CircularServer` — the table is cut into chunks that batched launches visit in
   a cycle; admitted queries join at the next launch and finish after one lap, so a
   query waits about one scan instead of the batch in progress plus its own.
+* :class:`PlannerRouter` — the learned planner (or the analytic model) on the serving
+  path: over a date-sorted table, an arriving query whose candidate segments the host
+  cores can answer sooner than the GPU's queue would (predicted CPU ms plus the CPU
+  queue's backlog, against the GPU latency the server is currently seeing) is answered
+  by the CPU engine from the pinned host columns instead of joining a GPU batch, which
+  also takes its work off the saturated GPU.
 """
 from __future__ import annotations
 
 import collections
 import ctypes as C
 import math
+import queue
 import statistics
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -102,6 +110,7 @@ class ServeReport:
     deferred: int = 0
     peak_held_bytes: int = 0
     scan_rows: int = 0          # fact rows the launches scanned
+    cpu_answered: int = 0       # queries the router sent to the host cores
 
     def summary(self, rows: int) -> dict:
         lat = sorted(self.latencies_ms)
@@ -114,7 +123,132 @@ class ServeReport:
                 "fact_rows_per_s": (self.scan_rows or self.batches * rows) / self.seconds if self.seconds else None,
                 "query_rows_per_s": len(lat) * rows / self.seconds if self.seconds else None,
                 "rejected": self.rejected, "deferred_admissions": self.deferred,
-                "peak_admitted_bytes": self.peak_held_bytes}
+                "peak_admitted_bytes": self.peak_held_bytes, "cpu_answered": self.cpu_answered}
+
+
+def _drain_cpu(router, rep: ServeReport, results: dict, queries, arrivals, t0: float, keep: bool) -> int:
+    """Record the queries the router's CPU worker has finished; returns how many."""
+    n = 0
+    while router is not None:
+        try:
+            qid, res, tdone = router.done.get_nowait()
+        except queue.Empty:
+            break
+        rep.latencies_ms.append((tdone - t0 - arrivals[qid]) * 1e3)
+        rep.cpu_answered += 1
+        if keep:
+            results[qid] = res.view(np.int64).copy() if queries[qid].template == "agg" else res
+        n += 1
+    return n
+
+
+def _arrive(ac, router, qid: int, q, nbytes: int) -> None:
+    if router is None or not router.route(qid, q):
+        ac.arrive(qid, nbytes)
+
+
+class _AllResident:
+    """The residency view of a table whose columns all live on the GPU."""
+
+    def __init__(self, nseg: int, ncol: int):
+        self.num_slots = nseg * ncol
+        self._idx = np.zeros(nseg, np.int32)
+
+    def col_idx(self, col: int) -> np.ndarray:
+        return self._idx
+
+    def stats(self) -> dict:
+        return {"resident": self.num_slots}
+
+
+class PlannerRouter:
+    """Sends an arriving query to the host cores when the planner predicts they answer it
+    sooner than the GPU path: predicted CPU ms over its candidate segments (segment
+    skipping on the date-sorted table) plus the CPU queue's predicted backlog, against
+    `margin` x the GPU latency the server has been seeing (a running median of recent GPU
+    completions). The CPU side is one worker thread running queries one at a time on the
+    CPU engine (mb_cpu_star_query over the pinned host columns, all host threads); its
+    results equal the GPU's (integer sums; rows outside the candidate segments cannot
+    match the query's date range)."""
+
+    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0):
+        from .engine import FACT, CpuShare, host_tables
+
+        class _Share(CpuShare):
+            pass
+
+        self.share = _Share()
+        self.share.t = table
+        self.share.hht = host_tables(table.sizes)
+        self.share.cache = _AllResident(table.nseg, len(FACT))
+        from . import cpu as _cpu
+        self.share.cpu_threads = _cpu.threads()
+        self.planner = planner
+        self.margin = margin
+        self.max_backlog_ms = max_backlog_ms
+        self.gpu_lat = collections.deque(maxlen=64)
+        self.backlog_ms = 0.0
+        self.q: queue.Queue = queue.Queue()
+        self.done: queue.Queue = queue.Queue()
+        self.routed = 0
+        self.considered = 0
+        self.pred_ms: list[float] = []
+        self.cpu_ms: list[float] = []
+        self._lock = threading.Lock()
+        self._th = threading.Thread(target=self._worker, daemon=True)
+        self._th.start()
+
+    def note_gpu_latency(self, ms: float) -> None:
+        self.gpu_lat.append(ms)
+
+    def route(self, qid: int, q: B.Query) -> bool:
+        """True when q was queued for the CPU (its result arrives through `done`)."""
+        self.considered += 1
+        if len(self.gpu_lat) < 8:
+            return False  # no GPU latency seen yet
+        cand = self.share.candidates(q)
+        if len(cand) == 0:
+            pred = 0.0
+        else:
+            pc, pg, fc, fg = self.planner.predict(self.share.context(q, cand))
+            pred = float(np.sum(pc) + fc)
+        gpu_now = float(np.median(self.gpu_lat))
+        with self._lock:
+            if self.backlog_ms + pred > min(self.margin * gpu_now, self.max_backlog_ms):
+                return False
+            self.backlog_ms += pred
+        self.routed += 1
+        self.q.put((qid, q, cand, pred))
+        return True
+
+    def _worker(self) -> None:
+        while True:
+            item = self.q.get()
+            if item is None:
+                return
+            qid, q, cand, pred = item
+            c0 = time.perf_counter()
+            res = np.zeros(2 if q.template == "agg" else 4 * q.groups, np.int32)
+            if len(cand):
+                self.share.build_cpu(q)
+                self.share._cpu_segments(q, [int(x) for x in cand], res)
+            ms = (time.perf_counter() - c0) * 1e3
+            with self._lock:
+                self.backlog_ms = max(0.0, self.backlog_ms - pred)
+                self.pred_ms.append(pred)
+                self.cpu_ms.append(ms)
+            self.done.put((qid, res, time.perf_counter()))
+
+    def close(self) -> None:
+        self.q.put(None)
+        self._th.join(timeout=60)
+
+    def summary(self) -> dict:
+        err = [abs(math.log(max(p, 1e-3)) - math.log(max(m, 1e-3))) for p, m in zip(self.pred_ms, self.cpu_ms)]
+        return {"planner": getattr(self.planner, "name", "?"), "routed_to_cpu": self.routed,
+                "considered": self.considered,
+                "cpu_ms_mean": statistics.mean(self.cpu_ms) if self.cpu_ms else None,
+                "mae_log_ms_cpu_prediction": statistics.mean(err) if err else None}
 
 
 class Server:
@@ -139,8 +273,9 @@ class Server:
         return out
 
     def serve(self, queries: list[B.Query], arrivals: np.ndarray, max_wait_s: float = 60.0,
-              keep_results: bool = False) -> tuple[ServeReport, dict]:
-        """Serve `queries` arriving at `arrivals` (s, ascending) in real time."""
+              keep_results: bool = False, router: "PlannerRouter | None" = None) -> tuple[ServeReport, dict]:
+        """Serve `queries` arriving at `arrivals` (s, ascending) in real time; with a router,
+        queries it sends to the host cores bypass the GPU batches."""
         ac = AdmissionController(self.budget)
         rep = ServeReport(len(queries), 0.0)
         results = {}
@@ -151,8 +286,9 @@ class Server:
         while done + ac.rejected < len(queries):
             now = time.perf_counter() - t0
             while i < len(queries) and arrivals[i] <= now:
-                ac.arrive(i, nbytes[i])
+                _arrive(ac, router, i, queries[i], nbytes[i])
                 i += 1
+            done += _drain_cpu(router, rep, results, queries, arrivals, t0, keep_results)
             rep.peak_held_bytes = max(rep.peak_held_bytes, ac.held)
             batch = ac.take(self.max_batch)
             if not batch:
@@ -161,6 +297,7 @@ class Server:
                     continue
                 if now > max_wait_s:
                     break
+                time.sleep(0.0002)  # only CPU-routed queries are outstanding
                 continue
             b0 = time.perf_counter()
             res = self.run_batch([queries[qid] for qid, _ in batch])
@@ -170,6 +307,8 @@ class Server:
             rep.batch_ms.append((time.perf_counter() - b0) * 1e3)
             for (qid, nb), r in zip(batch, res):
                 rep.latencies_ms.append((end - arrivals[qid]) * 1e3)
+                if router is not None:
+                    router.note_gpu_latency((end - arrivals[qid]) * 1e3)
                 if keep_results:
                     results[qid] = r
                 ac.release(nb)
@@ -199,8 +338,12 @@ class CircularServer:
     those of the query run alone. Up to 256 queries share a launch; a second launch is
     queued before the first completes so the GPU never waits for the host."""
 
+    # At most 128 queries share a launch: a batch of up to 128 carries 4 words of query mask
+    # per attribute value, more than 128 carry 8, and every row's mask work doubles — under a
+    # burst that slows every launch of the lap the burst joins, which lets the active set grow
+    # further. Queries beyond the cap wait in arrival order for the next launch.
     def __init__(self, t: dict, sizes: ssb.Sizes, n_rows: int, budget_bytes: int = 16 << 30,
-                 max_active: int = L.MB_BATCH_MAX_QUERIES, chunks: int = 8):
+                 max_active: int = 128, chunks: int = 8):
         self.t, self.sizes, self.n = t, sizes, n_rows
         self.pats = B.build_pats(t, sizes)
         self.dims = self.pats.c_dims()
@@ -231,8 +374,9 @@ class CircularServer:
         L.check("mb_batch_run", L.lib().mb_batch_run(C.byref(a), ssb._stream()))
 
     def serve(self, queries: list[B.Query], arrivals: np.ndarray, max_wait_s: float = 60.0,
-              keep_results: bool = False) -> tuple[ServeReport, dict]:
-        """Serve `queries` arriving at `arrivals` (s, ascending) in real time."""
+              keep_results: bool = False, router: "PlannerRouter | None" = None) -> tuple[ServeReport, dict]:
+        """Serve `queries` arriving at `arrivals` (s, ascending) in real time; with a router,
+        queries it sends to the host cores bypass the scan."""
         ac = AdmissionController(self.budget)
         rep = ServeReport(len(queries), 0.0)
         results = {}
@@ -247,8 +391,9 @@ class CircularServer:
         while done + ac.rejected < len(queries):
             now = time.perf_counter() - t0
             while i < len(queries) and arrivals[i] <= now:
-                ac.arrive(i, nbytes[i])
+                _arrive(ac, router, i, queries[i], nbytes[i])
                 i += 1
+            done += _drain_cpu(router, rep, results, queries, arrivals, t0, keep_results)
             for qid, nb in ac.take(self.max_active - len(active)):
                 res = queries[qid].result_buffer()
                 active.append(_Member(qid, nb, queries[qid], queries[qid].to_c(res), res))
@@ -285,6 +430,8 @@ class CircularServer:
                                 np.int64 if m.query.template == "agg" else np.int32).copy()
                         off += nb
                         rep.latencies_ms.append((end - arrivals[m.qid]) * 1e3)
+                        if router is not None:
+                            router.note_gpu_latency((end - arrivals[m.qid]) * 1e3)
                         ac.release(m.nbytes)
                     done += len(finishing)
                 continue
@@ -292,6 +439,8 @@ class CircularServer:
                 time.sleep(max(0.0, min(arrivals[i] - now, 0.001)))
             elif now > max_wait_s:
                 break
+            else:
+                time.sleep(0.0002)  # only CPU-routed queries are outstanding
         rep.seconds = time.perf_counter() - t0
         rep.rejected, rep.deferred = ac.rejected, ac.deferred
         return rep, results

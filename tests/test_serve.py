@@ -89,3 +89,52 @@ def test_circular_server_answers_every_query_exactly(chunks):
         B.run_alone(t, ws, qs[qid], r, n)
         assert np.array_equal(res[qid].reshape(-1), r.cpu().numpy().reshape(-1)), qid
     assert L.device_status(0) == 0
+
+
+class _CheapCpu:
+    """A planner stub predicting 0.1 ms of CPU work per segment (routes what it can)."""
+    name = "stub"
+
+    def predict(self, ctx):
+        n = len(ctx)
+        return np.full(n, 0.1), np.full(n, 1.0), 0.2, 0.0
+
+
+def test_router_prefers_the_gpu_until_it_has_seen_gpu_latencies():
+    r = S.PlannerRouter.__new__(S.PlannerRouter)
+    r.gpu_lat = __import__("collections").deque(maxlen=64)
+    r.considered = 0
+    assert not r.route(0, B.generate_queries(1, seed=1)[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("server", ["whole", "circular"])
+def test_router_sends_queries_to_the_cpu_with_exact_results(server):
+    """Over a date-sorted resident table, the router answers some queries on the host
+    cores (candidate segments only); every query's result equals its run alone."""
+    import torch
+    from mordred_b200 import _lib as L
+    from mordred_b200 import ssb
+    from mordred_b200.engine import SegmentedTable
+    torch.cuda.set_device(0)
+    n = 6 * (1 << 20) + 777
+    sizes = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    table = SegmentedTable(n, 31, sizes)
+    t = {k: torch.from_numpy(table.host[k]).cuda() for k in B.BATCH_FACT}
+    t.update(table.dims)
+    t.update(ssb.gen_device(sizes, 31, [], [d for d in B.BATCH_DIMS if d not in t]))
+    srv = S.Server(t, sizes, n, budget_bytes=4 << 20, max_batch=64) if server == "whole" else \
+        S.CircularServer(t, sizes, n, budget_bytes=4 << 20, max_active=64, chunks=4)
+    qs = B.generate_queries(240, seed=12, sel_lo=1e-4, sel_hi=0.3)
+    arr = S.poisson_arrivals(1500.0, len(qs), 13)
+    router = S.PlannerRouter(table, _CheapCpu(), margin=1.0, max_backlog_ms=1e9)
+    rep, res = srv.serve(qs, arr, keep_results=True, router=router)
+    router.close()
+    s = rep.summary(n)
+    assert s["completed"] == 240 and rep.cpu_answered > 10 and rep.cpu_answered < 240
+    ws = B.AloneWorkspace(sizes)
+    for qid in range(240):
+        r = qs[qid].result_buffer()
+        B.run_alone(t, ws, qs[qid], r, n)
+        assert np.array_equal(np.asarray(res[qid]).reshape(-1).view(np.int32), r.cpu().numpy().reshape(-1).view(np.int32)), qid
+    assert L.device_status(0) == 0
