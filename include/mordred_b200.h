@@ -138,6 +138,11 @@ typedef struct mb_star_args {
    * the engine kernels (src/gpudb/GPUProcessing.h:157-273, 393-494, 1385-1524, 1610-1846).
    * The launch fields above are ignored for a list. */
   const int* rows;
+  /* Cluster-resident mirrors of the sparse phase's hash tables (a presence bit, or a 4-bit
+   * payload code, per slot, spread over the shared memory of a cluster of CTAs, so those
+   * probes read on-chip memory instead of L2): 0 = the tuned default for the shape (large
+   * calls only), 1 = never, 2 = whenever the tables fit. Results are the same either way. */
+  int mirrors;
 } mb_star_args;
 
 /* Fused filter -> chained probe -> group-by/aggregate over the fact table.

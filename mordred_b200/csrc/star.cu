@@ -21,13 +21,16 @@ const Variant* star_variants_generic(int* count) {
   return kGeneric;
 }
 
-// The specialised variant for this shape if one was compiled, else the generic one.
-static const Variant* find_variant(int warps, int items, int nf, int nd, int ns) {
+// The specialised variant for this shape if one was compiled, else the generic one. The
+// mirror-reading variants exist for specialised shapes only.
+static const Variant* find_variant(int warps, int items, int nf, int nd, int ns, bool mir) {
   int n = 0;
   const Variant* sp = star_variants_special(&n);
   for (int i = 0; i < n; ++i)
-    if (sp[i].warps == warps && sp[i].items == items && sp[i].nf == nf && sp[i].nd == nd && sp[i].ns == ns)
+    if (sp[i].warps == warps && sp[i].items == items && sp[i].nf == nf && sp[i].nd == nd && sp[i].ns == ns &&
+        sp[i].mir == mir)
       return &sp[i];
+  if (mir) return nullptr;
   const Variant* g = star_variants_generic(&n);
   for (int i = 0; i < n; ++i)
     if (g[i].warps == warps && g[i].items == items) return &g[i];
@@ -56,7 +59,8 @@ static int add_col(StarPlan& P, const int* c) {
 
 static int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
-// Lay out shared memory for `stages` stages; returns total bytes.
+// Lay out shared memory for `stages` stages; returns total bytes. A mirror share (P.cluster >
+// 1) sits between the survivor lists and the stage ring.
 static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_bitmaps) {
   const int tile = ncw * 32 * items;
   int off = 2 * kMaxStages * 8;  // full and empty mbarriers
@@ -105,12 +109,67 @@ static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_b
   off = round_up(off, 16);
   P.smem_list_off = off;
   off += ncw * 32 * items * 2;
+  off = round_up(off, 16);
+  P.smem_mirror_off = off;
+  if (P.cluster > 1) off += 4 << P.mir_shift;
   off = round_up(off, 128);
   P.smem_stage_off = off;
   P.stage_bytes = P.ncols * tile * 4;
   P.stages = stages;
   P.smem_total = off + stages * P.stage_bytes;
   return P.smem_total;
+}
+
+// Plan cluster-resident mirrors for the sparse phase's table probes (those without a staged
+// bitmap): presence bits, or 4-bit payload codes when the probe's payload is read and its
+// group term leaves at most 14 payload values (the next larger group multiplier, or the
+// group count, over its own). Chooses the cluster size and the per-CTA share; returns false
+// (and clears the plan) when no probe qualifies or the mirrors do not fit.
+static bool plan_mirrors(StarPlan& P) {
+  P.cluster = 1;
+  P.mir_shift = 0;
+  long long words = 0;
+  bool any = false;
+  for (int p = 0; p < P.np; ++p) {
+    P.mir_kind[p] = kMirNone;
+    P.mir_base[p] = P.mir_words[p] = P.mir_min[p] = P.mir_payload[p] = 0;
+  }
+  for (int p = P.sparse_p0; p < P.np; ++p) {
+    if (P.p_bm_off[p] >= 0) continue;  // probed against its staged bitmap already
+    const bool need = !(P.p_layout[p] == MB_HT_KEY || (P.p_mul[p] == 0 && P.p_res_slot[p] < 0)) ||
+                      (p == 0 && P.agg_op == MB_AGG_MUL_PAYLOAD);
+    int kind = kMirBits;
+    if (need && P.p_layout[p] != MB_HT_KEY) {
+      // payload values the group term can tell apart: next multiplier above this one's, over it
+      long long next = P.gmode == kGroupScalar ? 1 : P.total_val;
+      for (int o = 0; o < P.np; ++o)
+        if (o != p && P.p_mul[o] > P.p_mul[p] && P.p_mul[o] < next) next = P.p_mul[o];
+      if (P.p_mul[p] > 0 && P.p_res_slot[p] >= 0 && next / P.p_mul[p] <= 14) kind = kMirNibble;
+    }
+    const long long w = kind == kMirNibble ? (P.p_slots[p] + 7ll) / 8 : (P.p_slots[p] + 31ll) / 32;
+    if (words + w > static_cast<long long>(kMirrorMaxCluster) * kMirrorMaxShareWords) continue;
+    P.mir_kind[p] = kind;
+    P.mir_base[p] = static_cast<int>(words);
+    P.mir_words[p] = static_cast<int>(w);
+    P.mir_min[p] = P.p_min[p];
+    P.mir_payload[p] = need ? 1 : 0;
+    words += w;
+    any = true;
+  }
+  if (!any) return false;
+  // the smallest share that fits with the portable cluster size, clusters of 8 (shares of
+  // at most kMirrorMaxShareWords); smaller shares leave more shared memory for stages
+  int shift = 0;
+  while ((static_cast<long long>(kMirrorMaxCluster) << shift) < words) ++shift;
+  P.cluster = kMirrorMaxCluster;
+  P.mir_shift = shift;
+  return true;
+}
+
+static void clear_mirrors(StarPlan& P) {
+  P.cluster = 1;
+  P.mir_shift = 0;
+  for (int p = 0; p < MB_MAX_PROBES; ++p) P.mir_kind[p] = kMirNone;
 }
 
 int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const DeviceState* preset) {
@@ -222,21 +281,73 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
     P.gmode = P.total_val <= kSmemGroupMax ? kGroupSmem : kGroupGlobal;
   if (group_mode == 1 && P.gmode != kGroupSmem) return MB_ERR_SIZE;
 
+  if (a->mirrors < 0 || a->mirrors > 2) return MB_ERR_ARG;
   const int budget = ds->max_smem_optin - 2048 - 2 * 8 * (ncw + 1);
   const int want_stages = a->stages ? a->stages : tc.stages;
   if (want_stages < 2 || want_stages > kMaxStages) return MB_ERR_ARG;
-  int smem = layout_smem(P, ncw, items, want_stages, true);
-  while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);
-  if (smem > budget && P.gmode == kGroupSmem && group_mode != 1) {
-    P.gmode = kGroupGlobal;
-    smem = layout_smem(P, ncw, items, want_stages, true);
+  clear_mirrors(P);
+  auto fit = [&]() -> int {
+    int smem = layout_smem(P, ncw, items, want_stages, true);
     while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);
+    if (smem > budget && P.gmode == kGroupSmem && group_mode != 1) {
+      P.gmode = kGroupGlobal;
+      smem = layout_smem(P, ncw, items, want_stages, true);
+      while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);
+    }
+    return smem;
+  };
+  int smem = fit();
+  // cluster-resident mirrors: on request (mirrors = 2), or by default for large calls with
+  // tiles; the plan needs the staged bitmaps laid out first, then the layout is redone
+  // with the mirror share
+  const bool try_mir = use_tiles && P.nfull > 0 && a->mirrors != 1 &&
+                       (a->mirrors == 2 || (tc.mirrors && P.n >= kMirrorMinRows)) && preset == nullptr;
+  const Variant* var = nullptr;
+  if (try_mir && smem <= budget && plan_mirrors(P)) {
+    const GroupMode keep_gmode = static_cast<GroupMode>(P.gmode);
+    smem = fit();
+    var = smem <= budget ? find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, true) : nullptr;
+    if (var == nullptr) {
+      clear_mirrors(P);
+      P.gmode = keep_gmode;
+      smem = fit();
+    }
   }
   if (smem > budget) smem = layout_smem(P, ncw, items, 2, false);
   if (smem > budget) return MB_ERR_SIZE;
-
-  const Variant* var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0);
+  if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false);
   if (var == nullptr) return MB_ERR_ARG;
+
+  long long want = P.nfull > 0 ? P.nfull : (P.n + threads - 1) / threads;
+  if (want < 1) want = 1;
+  if (var->mir) {
+    // one cluster of P.cluster CTAs per group of SMs; every CTA of a cluster holds a share
+    // of the mirrors, so the grid is whole clusters (CTAs without tiles still hold one)
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(P.cluster);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(threads + 32);
+    cfg.dynamicSmemBytes = static_cast<size_t>(smem);
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = a->grid > 0 ? (a->grid + P.cluster - 1) / P.cluster : 0;
+    if (clusters <= 0) {
+      cfg.gridDim = dim3(static_cast<unsigned>(P.cluster * 64));
+      if (cudaOccupancyMaxActiveClusters(&clusters, reinterpret_cast<const void*>(var->fn), &cfg) != cudaSuccess)
+        return MB_ERR_CUDA;
+      if (clusters < 1) return MB_ERR_SIZE;
+    }
+    const long long need_clusters = (want + P.cluster - 1) / P.cluster;
+    if (clusters > need_clusters) clusters = static_cast<int>(need_clusters);
+    cfg.gridDim = dim3(static_cast<unsigned>(clusters * P.cluster));
+    if (cudaLaunchKernelEx(&cfg, var->fn, P) != cudaSuccess) return MB_ERR_LAUNCH;
+    note_launches(1);
+    return MB_OK;
+  }
 
   int grid = a->grid;
   if (grid <= 0) {
@@ -246,8 +357,6 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
     if (per_sm < 1) per_sm = 1;
     grid = ds->num_sms * per_sm;
   }
-  long long want = P.nfull > 0 ? P.nfull : (P.n + threads - 1) / threads;
-  if (want < 1) want = 1;
   if (grid > want) grid = static_cast<int>(want);
 
   var->fn<<<grid, threads + 32, smem, stream>>>(P);

@@ -29,6 +29,16 @@ constexpr int kSmemGroupMax = 8192;            // groups kept in shared memory p
 constexpr int kBitmapSmemMaxBytes = 32768;     // largest presence bitmap staged (262,144 slots)
 constexpr int kBitmapSmemTotalBytes = 40960;
 constexpr int kBitmapDeriveMaxSlots8 = 65536;  // largest 8-byte-slot table whose bitmap a CTA derives
+// Cluster-resident mirrors: narrow copies of the sparse phase's hash tables (1 presence bit
+// or one 4-bit payload code per slot) spread over the shared memory of a thread-block
+// cluster, each CTA holding a power-of-two share of at most this many 32-bit words.
+constexpr int kMirrorMaxShareWords = 16384;   // 64 KB per CTA
+constexpr int kMirrorMaxCluster = 8;           // portable cluster size
+constexpr long long kMirrorMinRows = 8ll << 20;  // smaller calls do not repay building the mirrors
+enum MirrorKind { kMirNone = 0, kMirBits = 1, kMirNibble = 2 };
+// 4-bit payload codes: 0 absent, 1..14 present with payload min + code - 1, 15 present
+// with a payload the code cannot hold (read the table itself).
+constexpr unsigned kNibbleEscape = 15u;
 
 enum GroupMode { kGroupScalar = 0, kGroupSmem = 1, kGroupGlobal = 2 };
 
@@ -67,6 +77,14 @@ struct StarPlan {
   unsigned int* status;
   int stages;
   int smem_groups_off, smem_list_off, smem_stage_off, stage_bytes, smem_total;
+  // cluster-resident mirrors (cluster > 1): probe p's mirror kind, its first word in the
+  // cluster's word space, and the payload its codes count from; word w lives in CTA
+  // w >> mir_shift at share word w & ((1 << mir_shift) - 1)
+  int cluster;
+  int mir_kind[MB_MAX_PROBES], mir_base[MB_MAX_PROBES], mir_words[MB_MAX_PROBES], mir_min[MB_MAX_PROBES];
+  int mir_payload[MB_MAX_PROBES];  // 1: the probe's payload is read (from its code, else from the table)
+  int mir_shift;
+  int smem_mirror_off;
 };
 
 // Host: validate `a`, fill `plan`, pick the kernel variant and launch it on `stream`.

@@ -22,6 +22,7 @@ using KernelFn = void (*)(StarPlan);
 struct Variant {
   int warps, items, nf, nd, ns;
   KernelFn fn;
+  bool mir = false;  // reads cluster-resident mirrors (launched with a cluster)
 };
 
 __device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
@@ -48,6 +49,100 @@ __device__ __forceinline__ bool aligned16_dev(const void* p) { return (reinterpr
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// ---- thread-block clusters: rank, barrier, distributed shared memory ---------------------
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// Every thread of every CTA of the cluster arrives (its shared-memory writes released) and
+// waits for all (acquiring theirs). Warp-convergent: all lanes execute it together.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// 32-bit word at shared-memory address `local` (this CTA's address space) of cluster CTA `rank`.
+__device__ __forceinline__ uint32_t ld_dsmem_u32(uint32_t local, uint32_t rank) {
+  uint32_t remote, v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(remote));
+  return v;
+}
+
+// Word `rel` of probe p's mirror, computed from its hash table: 32 presence bits (slots
+// 32 * rel ..) or eight 4-bit payload codes (slots 8 * rel ..); slots past the table are 0.
+__device__ __forceinline__ uint32_t mirror_word(const StarPlan& P, int p, int rel) {
+  const int slots = P.p_slots[p];
+  const int* ht = P.p_ht[p];
+  uint32_t w = 0;
+  if (P.mir_kind[p] == kMirBits) {
+    const int s0 = rel * 32;
+    if (P.p_layout[p] == MB_HT_KEY) {
+      if (s0 + 32 <= slots && aligned16_dev(ht)) {
+        const int4* src = reinterpret_cast<const int4*>(ht + s0);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int4 q = __ldg(src + j);
+          w |= ((q.x != 0 ? 1u : 0u) << (4 * j)) | ((q.y != 0 ? 1u : 0u) << (4 * j + 1)) |
+               ((q.z != 0 ? 1u : 0u) << (4 * j + 2)) | ((q.w != 0 ? 1u : 0u) << (4 * j + 3));
+        }
+      } else {
+        for (int j = 0; j < 32 && s0 + j < slots; ++j) w |= (__ldg(ht + s0 + j) != 0 ? 1u : 0u) << j;
+      }
+    } else {
+      const unsigned long long* t8 = reinterpret_cast<const unsigned long long*>(ht);
+      if (s0 + 32 <= slots && aligned16_dev(ht)) {
+        const ulonglong2* src = reinterpret_cast<const ulonglong2*>(t8 + s0);
+#pragma unroll 4
+        for (int j = 0; j < 16; ++j) {
+          const ulonglong2 q = __ldg(src + j);
+          w |= ((q.x != 0ull ? 1u : 0u) << (2 * j)) | ((q.y != 0ull ? 1u : 0u) << (2 * j + 1));
+        }
+      } else {
+        for (int j = 0; j < 32 && s0 + j < slots; ++j) w |= (__ldg(t8 + s0 + j) != 0ull ? 1u : 0u) << j;
+      }
+    }
+    return w;
+  }
+  // payload codes: 0 absent, 1..14 payload - min + 1, 15 present with another payload
+  const int s0 = rel * 8;
+  const unsigned long long* t8 = reinterpret_cast<const unsigned long long*>(ht);
+  const bool hi = P.p_layout[p] == MB_HT_KEY_VAL;
+  const unsigned mn = static_cast<unsigned>(P.mir_min[p]);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    if (s0 + j >= slots) break;
+    const unsigned long long v = __ldg(t8 + s0 + j);
+    if (v == 0ull) continue;
+    const unsigned pay = hi ? static_cast<unsigned>(v >> 32) : static_cast<unsigned>(v);
+    const unsigned d = pay - mn;
+    const unsigned code = d <= 13u ? d + 1u : kNibbleEscape;
+    w |= code << (4 * j);
+  }
+  return w;
+}
+
+// This CTA's share of the cluster's mirror space (words rank << mir_shift ..), written by
+// `nthreads` threads numbered t.
+__device__ __forceinline__ void build_mirror_share(const StarPlan& P, uint32_t* share, int t, int nthreads) {
+  const int words = 1 << P.mir_shift;
+  const int w0 = static_cast<int>(cluster_rank()) << P.mir_shift;
+  for (int i = t; i < words; i += nthreads) {
+    const int gw = w0 + i;
+    uint32_t word = 0;
+    for (int p = 0; p < P.np; ++p) {
+      if (P.mir_kind[p] == kMirNone) continue;
+      const int rel = gw - P.mir_base[p];
+      if (rel >= 0 && rel < P.mir_words[p]) {
+        word = mirror_word(P, p, rel);
+        break;
+      }
+    }
+    share[i] = word;
+  }
 }
 
 // Column pointer for row `r` of this call (direct or through the segment cache).
@@ -247,6 +342,122 @@ __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint
   aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
 }
 
+// The sparse phase with cluster-resident mirrors: a probe with a mirror tests presence —
+// and, with payload codes, reads the payload — in the cluster's distributed shared memory
+// instead of L2; probes without one read their tables as in sparse_rows. Payloads a mirror
+// does not hold (presence-bit mirrors of tables whose payload is read, escaped codes) are
+// read from the table for the rows that survive every probe. Selection, payloads and
+// status bits equal the sequential chain's.
+template <int NSC, class L>
+__device__ __forceinline__ void sparse_rows_mir(const StarPlan& P, const L& ld, uint32_t sel, int p0, int ns,
+                                                unsigned bias, Accum& A, unsigned long long* s_sum, uint32_t* s_touch,
+                                                const unsigned char* smem) {
+  constexpr int ITEMS = L::ITEMS;
+  if (sel == 0) return;
+  int v[ITEMS];
+  int gv[MB_MAX_PROBES][ITEMS];
+  unsigned long long sv[MB_MAX_PROBES][ITEMS];
+  uint32_t range_bad[MB_MAX_PROBES], absent[MB_MAX_PROBES], fetch[MB_MAX_PROBES];
+#pragma unroll
+  for (int p = 0; p < MB_MAX_PROBES; ++p) {
+    range_bad[p] = 0;
+    absent[p] = 0;
+    fetch[p] = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      gv[p][i] = 0;
+      sv[p][i] = 0;
+    }
+  }
+  const uint32_t share = smem_addr(smem + P.smem_mirror_off);
+  const int smask = (1 << P.mir_shift) - 1;
+  const int nsp = NSC >= 0 ? NSC : ns;
+#pragma unroll
+  for (int round = 0; round < 2; ++round) {
+    const int qlo = round == 0 ? 0 : 1, qhi = round == 0 ? 1 : MB_MAX_PROBES;
+#pragma unroll
+    for (int q = 0; q < MB_MAX_PROBES; ++q) {
+      if (q >= nsp) break;
+      if (q < qlo || q >= qhi) continue;
+      const int p = p0 + q;
+      ld.load(P.p_col[p], v);
+      const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p], kind = P.mir_kind[p];
+      const int base = P.mir_base[p];
+      const int* ht = P.p_ht[p];
+      const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i) {
+        if (!(sel & (1u << i))) continue;
+        const int h = pht_slot(v[i], slots, kmin);
+        if (h < 0) {
+          range_bad[q] |= 1u << i;
+        } else if (bm != nullptr && !((bm[h >> 5] >> (h & 31)) & 1u)) {
+          absent[q] |= 1u << i;
+        } else if (kind == kMirBits) {
+          const int gw = base + (h >> 5);
+          sv[q][i] = (ld_dsmem_u32(share + 4u * static_cast<uint32_t>(gw & smask), static_cast<uint32_t>(gw) >> P.mir_shift) >>
+                      (h & 31)) & 1u;
+        } else if (kind == kMirNibble) {
+          const int gw = base + (h >> 3);
+          sv[q][i] = (ld_dsmem_u32(share + 4u * static_cast<uint32_t>(gw & smask), static_cast<uint32_t>(gw) >> P.mir_shift) >>
+                      (4 * (h & 7))) & 15u;
+        } else if (layout == MB_HT_KEY) {
+          sv[q][i] = bm != nullptr ? 1ull : static_cast<unsigned long long>(static_cast<unsigned>(__ldg(ht + h)));
+        } else {
+          sv[q][i] = ldg_u64(ht + 2 * h);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < MB_MAX_PROBES; ++q) {
+      if (q >= nsp) break;
+      if (q < qlo || q >= qhi) continue;
+      const int p = p0 + q;
+      const int layout = P.p_layout[p], kind = P.mir_kind[p];
+#pragma unroll
+      for (int i = 0; i < ITEMS; ++i) {
+        if (!(sel & (1u << i))) continue;
+        if (range_bad[q] & (1u << i)) {
+          A.bad_probe = true;
+          sel &= ~(1u << i);
+        } else if ((absent[q] & (1u << i)) || sv[q][i] == 0) {
+          sel &= ~(1u << i);
+        } else if (kind == kMirBits) {
+          if (P.mir_payload[p]) fetch[q] |= 1u << i;
+        } else if (kind == kMirNibble) {
+          if (sv[q][i] == kNibbleEscape)
+            fetch[q] |= 1u << i;
+          else
+            gv[q][i] = static_cast<int>(static_cast<unsigned>(P.mir_min[p]) + static_cast<unsigned>(sv[q][i]) - 1u);
+        } else {
+          gv[q][i] = layout == MB_HT_KEY_VAL   ? static_cast<int>(sv[q][i] >> 32)
+                     : layout == MB_HT_VAL_OFF ? static_cast<int>(static_cast<unsigned>(sv[q][i]))
+                                               : 0;
+        }
+      }
+    }
+    if (sel == 0) return;  // per lane; nothing warp-wide follows
+  }
+  // payloads the mirrors do not hold, for the rows that passed every probe
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= nsp) break;
+    if (!(fetch[q] & sel)) continue;
+    const int p = p0 + q;
+    ld.load(P.p_col[p], v);
+    const int* ht = P.p_ht[p];
+    const bool hi = P.p_layout[p] == MB_HT_KEY_VAL;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      if (!(fetch[q] & sel & (1u << i))) continue;
+      const unsigned long long raw = ldg_u64(ht + 2 * pht_slot(v[i], P.p_slots[p], P.p_kmin[p]));
+      gv[q][i] = hi ? static_cast<int>(raw >> 32) : static_cast<int>(static_cast<unsigned>(raw));
+    }
+  }
+  if (P.count_after < 0) A.cnt += __popc(sel);
+  aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
+}
+
 // Dense phase over a warp's slice of a staged tile: lane l owns rows (j*32 + l)*4 + e,
 // read with 128-bit shared loads; applies every filter and the leading probes whose
 // presence bitmap is staged. Returns the selection (bit j*4 + e).
@@ -349,7 +560,7 @@ __device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& 
   sparse_rows<-1>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
 }
 
-template <int NCW, int ITEMS, int NFC, int NDC, int NSC>
+template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false>
 __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_constant__ StarPlan P) {
   constexpr int WROWS = 32 * ITEMS;
   constexpr int TILE = NCW * WROWS;
@@ -443,32 +654,49 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
 
   if (warp == 0) {
     // ---- producer: one lane streams tiles into the stage ring ----------------------
+    const uint64_t policy = l2_policy_evict_first();
+    long long k = 0;
+    int s = 0;
+    uint32_t phase = 0;  // use count of stage s, mod 2
+    auto issue = [&](long long kk, int ss) {
+      const long long r0 = (b + kk * G) * static_cast<long long>(TILE);
+      int* dst = stage_base + ss * stage_words;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&full[ss], stage_words * 4u);
+      if (P.gpu_cache == nullptr) {
+        for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, &full[ss], policy);
+      } else {
+        const long long vseg = r0 >> P.seg_shift;
+        const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg])
+                                    : static_cast<int>((P.start_offset + r0) >> P.seg_shift);
+        const long long in_seg = r0 & ((1ll << P.seg_shift) - 1);
+        for (int c = 0; c < P.ncols; ++c) {
+          const long long slot = P.col[c][seg];
+          bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, &full[ss], policy);
+        }
+      }
+    };
+    if (MIR) {
+      // fill the ring while the consumers build the mirrors, then join the cluster barrier
+      if (lane == 0) {
+        for (; k < my_tiles && k < S; ++k) {
+          issue(k, s);
+          if (++s == S) {
+            s = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      __syncwarp();
+      cluster_sync_all();
+    }
     if (lane == 0) {
-      const uint64_t policy = l2_policy_evict_first();
-      long long k = 0;
-      int s = 0;
-      uint32_t phase = 0;  // use count of stage s, mod 2
       for (; k < my_tiles; ++k) {
         if (k >= S && !mbar_wait_bounded(&empty[s], phase ^ 1u)) {
           failed = true;
           break;
         }
-        const long long r0 = (b + k * G) * static_cast<long long>(TILE);
-        int* dst = stage_base + s * stage_words;
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&full[s], stage_words * 4u);
-        if (P.gpu_cache == nullptr) {
-          for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, &full[s], policy);
-        } else {
-          const long long vseg = r0 >> P.seg_shift;
-          const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg])
-                                      : static_cast<int>((P.start_offset + r0) >> P.seg_shift);
-          const long long in_seg = r0 & ((1ll << P.seg_shift) - 1);
-          for (int c = 0; c < P.ncols; ++c) {
-            const long long slot = P.col[c][seg];
-            bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, &full[s], policy);
-          }
-        }
+        issue(k, s);
         if (++s == S) {
           s = 0;
           phase ^= 1u;
@@ -485,6 +713,12 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     const int nd = P.sparse_p0;  // the sparse phase starts at probe sparse_p0 <= n_dense
     const int ns = NSC >= 0 ? NSC : P.np - P.sparse_p0;
     const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
+    if (MIR) {
+      // this CTA's share of the mirrors, visible cluster-wide after the barrier
+      build_mirror_share(P, reinterpret_cast<uint32_t*>(smem + P.smem_mirror_off), tid - 32, NCW * 32);
+      __syncwarp();
+      cluster_sync_all();
+    }
     int s = 0;
     uint32_t phase = 0;
     for (long long k = 0; k < my_tiles; ++k) {
@@ -506,7 +740,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
           ld.r[i] = idx < total ? list[idx] : 0;
           if (idx < total) live |= 1u << i;
         }
-        sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+        if (MIR)
+          sparse_rows_mir<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+        else
+          sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
@@ -558,6 +795,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
   if (P.gmode == kGroupSmem) {
     for (int g = tid; g < P.total_val; g += NWARPS * 32)
       if ((s_touch[g >> 5] >> (g & 31)) & 1u) atomicAdd(group_sum_ptr(P, g), s_sum[g]);
+  }
+  if (MIR) {
+    // no CTA leaves while another may still read its share of the mirrors
+    __syncwarp();
+    cluster_sync_all();
   }
 }
 

@@ -9,6 +9,12 @@ namespace mb {
   {4, 16, NF, ND, NS, star_kernel<4, 16, NF, ND, NS>}, {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS>}, \
       {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS>}, {8, 16, NF, ND, NS, star_kernel<8, 16, NF, ND, NS>}
 
+// the same shapes reading cluster-resident mirrors in the sparse phase
+#define MB_MIRROR_VARIANTS(NF, ND, NS)                                                        \
+  {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS, true>, true},                              \
+      {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS, true>, true},                        \
+      {8, 16, NF, ND, NS, star_kernel<8, 16, NF, ND, NS, true>, true}
+
 static const Variant kSpecial[] = {
     MB_SHAPE_VARIANTS(3, 0, 0),  // filter-aggregate (q11.cu)
     MB_SHAPE_VARIANTS(0, 1, 2),  // Query A: supplier bitmap, part and date tables (q21.cu)
@@ -16,6 +22,10 @@ static const Variant kSpecial[] = {
     MB_SHAPE_VARIANTS(2, 1, 4),  // engine filter_probe_group_by: supplier bitmap, four tables
     MB_SHAPE_VARIANTS(0, 1, 4),  // engine probe_group_by: supplier bitmap, four tables
     MB_SHAPE_VARIANTS(0, 0, 1),  // src/ops probe, one table
+    MB_MIRROR_VARIANTS(0, 1, 2),
+    MB_MIRROR_VARIANTS(0, 1, 3),
+    MB_MIRROR_VARIANTS(2, 1, 4),
+    MB_MIRROR_VARIANTS(0, 1, 4),
 };
 
 const Variant* star_variants_special(int* count) {

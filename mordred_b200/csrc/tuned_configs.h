@@ -9,6 +9,7 @@ namespace mb {
 
 struct TunedConfig {
   int threads, items, stages, group_mode;
+  int mirrors = 0;  // 1: large calls of this shape use cluster-resident mirrors by default
 };
 
 struct TunedEntry {
