@@ -100,8 +100,9 @@ class BatchExecutor(CpuShare):
 
     # ---- planning ------------------------------------------------------------------------
     def _predict(self, planner, queries, cands):
-        """Per query: (cpu_ms, gpu_ms, cpu_fixed, gpu_fixed, gpu_ms if missing, gpu_ms if
-        resident) over its candidate segments, from one batched model call."""
+        """Per query, the planner's (cpu_ms, gpu_ms, cpu_fixed, gpu_fixed) over its candidate
+        segments, and — for admission — the predicted GPU ms each segment saves when its
+        columns are resident rather than missing (batched model calls)."""
         ctxs = [self.context(q, c) for q, c in zip(queries, cands)]
         base = planner.predict_many(ctxs)
         if not self.admission:
@@ -233,8 +234,10 @@ class BatchExecutor(CpuShare):
         gsegs, csegs = segs[on_gpu], segs[~on_gpu]
         plan_ms = (time.perf_counter() - t0) * 1e3
 
-        # result buffers and launch descriptors (chunks of up to 256 queries)
+        # result buffers (zeroed on the current stream, which the kernel stream then waits
+        # for) and launch descriptors (chunks of up to 256 queries)
         flat, views = B.result_buffers(queries)
+        ks.wait_stream(torch.cuda.current_stream())
         qarrs = []
         for base in range(0, len(queries), L.MB_BATCH_MAX_QUERIES):
             chunk = list(range(base, min(len(queries), base + L.MB_BATCH_MAX_QUERIES)))

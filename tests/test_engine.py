@@ -96,3 +96,30 @@ def test_learned_planner_trains_and_round_trips(tmp_path):
     p.save(str(tmp_path / "mlp.bin"), {"note": "test"})
     q = LearnedPlanner.load(str(tmp_path / "mlp.bin"))
     assert np.array_equal(q.predict_log(x[:50]), p.predict_log(x[:50]))
+
+
+def test_shipped_planner_weights_predict_better_than_the_analytic_model(setup):
+    """The trained planner (mordred_b200/planner_weights) on segments timed live here — the
+    method's measure of what the model gains over the analytic cost model it replaces:
+    its mean absolute error of log ms is below the analytic model's, for CPU and GPU."""
+    from mordred_b200 import planner_experiment as PE
+    from mordred_b200.planner import MIN_MS
+    t, ex, dev = setup
+    learned = LearnedPlanner.load(PE.DEFAULT_WEIGHTS)
+    rng = np.random.default_rng(5)
+    feats, truth, ana = [], [], []
+    for q in B.generate_queries(16, seed=2718):
+        cand = ex.candidates(q)
+        if len(cand) == 0:
+            continue
+        recs, _ = ex.profile_segments(q, rng.choice(cand, min(5, len(cand)), replace=False))
+        for r in recs:
+            feats.append(r["features"])
+            truth.append([r["cpu_ms"], r["gpu_ms"]])
+            ana.append([r["analytic_cpu_ms"], r["analytic_gpu_ms"]])
+    assert len(feats) >= 20
+    truth = np.log(np.maximum(np.array(truth), MIN_MS))
+    err_l = np.abs(learned.predict_log(np.stack(feats)) - truth).mean(0)
+    err_a = np.abs(np.log(np.maximum(np.array(ana), MIN_MS)) - truth).mean(0)
+    assert (err_l < err_a).all(), (err_l, err_a)
+    assert L.device_status(0) == 0
