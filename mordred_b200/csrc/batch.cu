@@ -124,6 +124,20 @@ __device__ __forceinline__ int bslot(int key, int slots, int kmin) {
   return d % slots;
 }
 
+// Physical tile of scan position t (CTA b takes positions b, b + G, b + 2G, ...). The
+// first kTileRegions * Q tiles (Q = nfull / kTileRegions) are visited column-major over
+// kTileRegions regions of the table, so the tiles the grid holds at one moment lie in
+// different regions rather than side by side. On a table sorted by date, side-by-side
+// tiles share a date: every SM would then add into the same queries' group records (the
+// same year's) at once, while the regions spread those updates over the table's years.
+// Every CTA still sees every region, so the work stays balanced.
+constexpr long long kTileRegions = 16;
+__device__ __forceinline__ long long tile_order(long long t, long long nfull) {
+  const long long q = nfull / kTileRegions;
+  if (t >= q * kTileRegions) return t;
+  return (t % kTileRegions) * q + t / kTileRegions;
+}
+
 __device__ __forceinline__ int field_value(int v, int code) {
   const int width = code & 63;
   const unsigned shift = (code >> 6) & 31;
@@ -337,7 +351,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
           failed = true;
           break;
         }
-        const long long r0 = (b + k * G) * static_cast<long long>(TILE);
+        const long long r0 = tile_order(b + k * G, P.nfull) * static_cast<long long>(TILE);
         int* dst = stage_base + s * P.stage_words;
         fence_proxy_async_smem();
         mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>(P.ncols) * TILE * 4u);

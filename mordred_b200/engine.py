@@ -155,6 +155,7 @@ class CpuShare:
 
     t: SegmentedTable
     hht: dict
+    cpu_nthreads: int = 0  # host threads of the CPU side (0: every thread of the engine's pool)
 
     def candidates(self, q: B.Query) -> np.ndarray:
         """Segments whose orderdate [min, max] meets the query's range (and, for the
@@ -174,21 +175,22 @@ class CpuShare:
         BT = L.MB_FILTER_BETWEEN
         h["s"][:] = 0
         h["d"][:] = 0
+        nt = self.cpu_nthreads
         cpu.build_pht(d["s_region"], BT, q.s_region[0], q.s_region[1], d["s_suppkey"], None, h["s"], s.s_len, 0,
-                      L.MB_HT_KEY)
+                      L.MB_HT_KEY, nt)
         cpu.build_pht(None, 0, 0, 0, d["d_datekey"], d["d_year"], h["d"], ssb.DATE_SLOTS, ssb.DATE_MIN,
-                      L.MB_HT_KEY_VAL)
+                      L.MB_HT_KEY_VAL, nt)
         if q.template == "qa":
             h["p_kv"][:] = 0
             cpu.build_pht(d["p_category"], BT, q.category[0], q.category[1], d["p_partkey"], d["p_brand1"], h["p_kv"],
-                          s.p_len, 0, L.MB_HT_KEY_VAL)
+                          s.p_len, 0, L.MB_HT_KEY_VAL, nt)
         else:
             h["c"][:] = 0
             h["p_key"][:] = 0
             cpu.build_pht(d["c_region"], BT, q.c_region[0], q.c_region[1], d["c_custkey"], d["c_nation"], h["c"],
-                          s.c_len, 0, L.MB_HT_KEY_VAL)
+                          s.c_len, 0, L.MB_HT_KEY_VAL, nt)
             cpu.build_pht(d["p_mfgr"], BT, q.mfgr[0], q.mfgr[1], d["p_partkey"], None, h["p_key"], s.p_len, 0,
-                          L.MB_HT_KEY)
+                          L.MB_HT_KEY, nt)
 
     def args(self, q: B.Query, col, ht: dict, n_rows: int, res, **extra) -> L.MbStarArgs:
         """mb_star_args of query q; col(name) gives a column (pointer or array), ht the tables."""
@@ -234,7 +236,7 @@ class CpuShare:
         group = segs.astype(np.int16)  # the arguments hold its address: keep it alive through the call
         a = self.args(q, lambda name: self.t.host[name], self.hht, self._rows(segs), res, segment_group=group,
                       segment_size=SEG)
-        cpu.star_query(a)
+        cpu.star_query(a, nthreads=self.cpu_nthreads)
 
     def context(self, q: B.Query, segs: np.ndarray) -> QueryContext:
         """The planners' view of q over `segs`: rows, in-range share of each segment's

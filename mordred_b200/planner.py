@@ -186,6 +186,39 @@ class LearnedPlanner:
         y = np.exp(self.predict_log(features(ctx)))
         return y[:, 0], y[:, 1], fc, fg
 
+    def predict_log_host(self, feats: np.ndarray) -> np.ndarray:
+        """The same network evaluated on the host (fp32, numpy). For callers that must not
+        wait on the device: a forward launch queues behind whatever occupies the SMs (a
+        persistent batch kernel holds every SM until it ends). Agrees with the kernel to
+        fp32 rounding (the summation order differs)."""
+        w = self._host_params()
+        x = (np.asarray(feats, np.float32) - self.mean) / self.std
+        h1 = np.maximum(x @ w["W1"] + w["b1"], 0.0)
+        h2 = np.maximum(h1 @ w["W2"] + w["b2"], 0.0)
+        return (h2 @ w["W3"] + w["b3"]).astype(np.float64)
+
+    def predict_host(self, ctx: QueryContext):
+        """predict() with the host forward pass."""
+        fc, fg = self.fixed_ms.get(ctx.template, [0.0, 0.0])
+        if len(ctx) == 0:
+            return np.zeros(0), np.zeros(0), fc, fg
+        y = np.exp(self.predict_log_host(features(ctx)))
+        return y[:, 0], y[:, 1], fc, fg
+
+    def _host_params(self) -> dict:
+        key = id(self.params), self.params._version
+        if getattr(self, "_host_key", None) != key:
+            p = self.params.detach().cpu().numpy()
+            i, h, o = L.MB_MLP_IN, L.MB_MLP_HIDDEN, L.MB_MLP_OUT
+            w, off = {}, 0
+            for name, shape in (("W1", (i, h)), ("b1", (h,)), ("W2", (h, h)), ("b2", (h,)), ("W3", (h, o)),
+                                ("b3", (o,))):
+                n = int(np.prod(shape))
+                w[name] = p[off: off + n].reshape(shape)
+                off += n
+            self._host_w, self._host_key = w, key
+        return self._host_w
+
     def predict_many(self, ctxs: list[QueryContext]) -> list:
         """predict() for many queries with one model call over all their segments."""
         feats = [features(c) for c in ctxs if len(c)]

@@ -167,11 +167,11 @@ class PlannerRouter:
     skipping on the date-sorted table) plus the CPU queue's predicted backlog, against
     `margin` x the GPU latency the server has been seeing (a running median of recent GPU
     completions). The CPU side is one worker thread running queries one at a time on the
-    CPU engine (mb_cpu_star_query over the pinned host columns, all host threads); its
-    results equal the GPU's (integer sums; rows outside the candidate segments cannot
-    match the query's date range)."""
+    CPU engine (mb_cpu_star_query over the pinned host columns, all host threads but
+    `spare_cores`); its results equal the GPU's (integer sums; rows outside the candidate
+    segments cannot match the query's date range)."""
 
-    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0):
+    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0, spare_cores: int = 2):
         from .engine import FACT, CpuShare, host_tables
 
         class _Share(CpuShare):
@@ -182,8 +182,13 @@ class PlannerRouter:
         self.share.hht = host_tables(table.sizes)
         self.share.cache = _AllResident(table.nseg, len(FACT))
         from . import cpu as _cpu
-        self.share.cpu_threads = _cpu.threads()
+        # the serving thread (planning, launches, result copies) keeps `spare_cores` cores:
+        # a CPU engine on every core slows the GPU path it is meant to relieve
+        self.share.cpu_nthreads = max(1, _cpu.threads() - spare_cores)
+        self.share.cpu_threads = self.share.cpu_nthreads
         self.planner = planner
+        # predictions on the host: a forward launch would queue behind the batch kernels
+        self._predict = getattr(planner, "predict_host", planner.predict)
         self.margin = margin
         self.max_backlog_ms = max_backlog_ms
         self.gpu_lat = collections.deque(maxlen=64)
@@ -210,7 +215,7 @@ class PlannerRouter:
         if len(cand) == 0:
             pred = 0.0
         else:
-            pc, pg, fc, fg = self.planner.predict(self.share.context(q, cand))
+            pc, pg, fc, fg = self._predict(self.share.context(q, cand))
             pred = float(np.sum(pc) + fc)
         gpu_now = float(np.median(self.gpu_lat))
         with self._lock:

@@ -90,3 +90,21 @@ def test_cuda_adam_and_training_reduce_loss():
         if first is None:
             first = loss.item()
     assert loss.item() < 0.1 * first
+
+
+def test_host_forward_matches_fp64_oracle():
+    """The planner's host forward pass (the serving router's path) against the oracle."""
+    from mordred_b200.planner import LearnedPlanner
+    p, x, _ = _case(77, 300)
+    pl = LearnedPlanner(params=p, device="cpu")
+    y = pl.predict_log_host(x)
+    y_ref, _ = M.forward(p.astype(np.float32).astype(np.float64), x.astype(np.float32).astype(np.float64))
+    assert np.allclose(y, y_ref, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_host_forward_matches_cuda_forward():
+    from mordred_b200.planner import LearnedPlanner
+    p, x, _ = _case(78, 500)
+    pl = LearnedPlanner(params=p)
+    assert np.allclose(pl.predict_log_host(x), pl.predict_log(x), rtol=1e-4, atol=1e-4)
