@@ -32,6 +32,7 @@ Results equal each query run alone (integer sums; tests/test_batch_engine.py).
 from __future__ import annotations
 
 import ctypes as C
+import queue
 import threading
 import time
 from dataclasses import dataclass, field
@@ -88,10 +89,18 @@ class BatchExecutor(CpuShare):
         self.kstream = torch.cuda.Stream()
         self.cstream = torch.cuda.Stream()
         self.max_waves = table.nseg // stage_segments + 3
-        self.col_h = torch.empty(self.max_waves, ncol, table.nseg, dtype=torch.int32, pin_memory=True)
+        # host slot arrays per window parity: a window's copies of them may still be queued
+        # behind the previous window's scans while the next window is being enqueued
+        self.col_h = torch.empty(2, self.max_waves, ncol, table.nseg, dtype=torch.int32, pin_memory=True)
         self.col_d = torch.empty(self.max_waves, ncol, table.nseg, dtype=torch.int32, device="cuda")
-        self.seg_h = torch.empty(self.max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
+        self.seg_h = torch.empty(2, self.max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
         self.seg_d = torch.empty(self.max_waves, table.nseg, dtype=torch.int16, device="cuda")
+        self._parity = 0
+        self._stage_done = [None, None]  # events: the last scans that read staging buffer 0 / 1
+        self._stage_buf = 0
+        self._cpu_jobs: queue.Queue = queue.Queue()
+        self._cpu_worker = threading.Thread(target=self._cpu_loop, daemon=True)
+        self._cpu_worker.start()
         self.ws = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
         self.host_ptrs = [table.ptr(c, 0) for c in FACT]
         self.benefit = np.zeros((ncol, table.nseg))
@@ -178,13 +187,14 @@ class BatchExecutor(CpuShare):
         for i in range(0, len(rest), self.stage_segments):
             waves.append((self._order(rest[i: i + self.stage_segments], self.t), True))
         launches, staged = 0, 0
-        done_ev = [None, None]     # kernels that last read staging buffer 0 / 1
-        buf = 0
+        done_ev = self._stage_done  # scans that last read staging buffer 0 / 1 (any window)
+        buf = self._stage_buf
+        col_h, seg_h = self.col_h[self._parity], self.seg_h[self._parity]
         for w, (segs, needs_stage) in enumerate(waves):
             if w >= self.max_waves:
                 raise RuntimeError("more waves than the executor's slot arrays hold")
             for c in cols_needed:
-                self.col_h[w, c, segs] = torch.from_numpy(idx[c][segs])
+                col_h[w, c, segs] = torch.from_numpy(idx[c][segs])
             if needs_stage:
                 if done_ev[buf] is not None:
                     cs.wait_event(done_ev[buf])
@@ -195,25 +205,43 @@ class BatchExecutor(CpuShare):
                         slot = self.stage0 + (buf * self.stage_segments + j) * len(FACT) + c
                         self.cache.stage(slot, self.host_ptrs[c] + int(s) * SEG * 4, int(self.t.seg_rows[s]),
                                          cs.cuda_stream)
-                        self.col_h[w, c, s] = slot
+                        col_h[w, c, s] = slot
                         staged += 1
                 copied = torch.cuda.Event()
                 copied.record(cs)
                 ks.wait_event(copied)
-            self.seg_h[w, : len(segs)] = torch.from_numpy(segs.astype(np.int16))
+            seg_h[w, : len(segs)] = torch.from_numpy(segs.astype(np.int16))
             with torch.cuda.stream(ks):
-                self.col_d[w].copy_(self.col_h[w], non_blocking=True)
-                self.seg_d[w, : len(segs)].copy_(self.seg_h[w, : len(segs)], non_blocking=True)
+                self.col_d[w].copy_(col_h[w], non_blocking=True)
+                self.seg_d[w, : len(segs)].copy_(seg_h[w, : len(segs)], non_blocking=True)
             launches += self._launch(w, segs, qarrs, cols_needed, ks)
             if needs_stage:
                 ev = torch.cuda.Event()
                 ev.record(ks)
                 done_ev[buf] = ev
                 buf ^= 1
+        self._stage_buf = buf
         return launches, len(waves), staged
 
     # ---- one window ---------------------------------------------------------------------------
-    def run_window(self, queries: list[B.Query], planner) -> WindowRun:
+    def _cpu_loop(self) -> None:
+        """The windows' CPU shares, one after another (they share the host hash tables)."""
+        while True:
+            job = self._cpu_jobs.get()
+            if job is None:
+                return
+            fn, done, err = job
+            try:
+                fn()
+            except BaseException as e:  # re-raised by _finish_window
+                err.append(e)
+            finally:
+                done.set()
+
+    def _start_window(self, queries: list[B.Query], planner) -> dict:
+        """Plan a window and enqueue all of its work: admission copies, staged waves and
+        scans on the device streams, its CPU share on the CPU worker. Returns what
+        _finish_window needs; nothing here waits for earlier windows' device work."""
         t0 = time.perf_counter()
         ks = self.kstream
         cands = [self.candidates(q) for q in queries]
@@ -246,7 +274,7 @@ class BatchExecutor(CpuShare):
             qarrs.append((arr, len(chunk), cols))
         cols_needed = sorted({c for _, _, cols in qarrs for c in cols})
 
-        # CPU share on its own thread: per query, its host tables and its CPU segments
+        # CPU share on the CPU worker: per query, its host tables and its CPU segments
         host_res = [np.zeros(2 if q.template == "agg" else 4 * q.groups, np.int32) for q in queries]
         cseg_set = set(int(s) for s in csegs)
         cpu_ms = [0.0]
@@ -260,31 +288,61 @@ class BatchExecutor(CpuShare):
                     self._cpu_segments(q, mine, host_res[qi])
             cpu_ms[0] = (time.perf_counter() - c0) * 1e3
 
-        th = threading.Thread(target=cpu_share) if len(csegs) else None
-        if th:
-            th.start()
+        cpu_done, cpu_err = threading.Event(), []
+        if len(csegs):
+            self._cpu_jobs.put((cpu_share, cpu_done, cpu_err))
+        else:
+            cpu_done.set()
         g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         g0.record(ks)
         launches, waves, staged = self._gpu_share(gsegs, qarrs, cols_needed)
         g1.record(ks)
+        self._parity ^= 1
         host = torch.empty(flat.numel(), dtype=torch.uint8, pin_memory=True)
         with torch.cuda.stream(ks):
             host.copy_(flat, non_blocking=True)
-        if th:
-            th.join()
-        ks.synchronize()
-        hb = host.numpy()
+        read = torch.cuda.Event()
+        read.record(ks)
+        return dict(t0=t0, queries=queries, segs=segs, gsegs=gsegs, csegs=csegs, span=span, plan_ms=plan_ms,
+                    copied=copied, flat=flat, qarrs=qarrs, host_res=host_res, cpu_ms=cpu_ms, cpu_done=cpu_done,
+                    cpu_err=cpu_err,
+                    g0=g0, g1=g1, launches=launches, waves=waves, staged=staged, host=host, read=read)
+
+    def _finish_window(self, st: dict) -> WindowRun:
+        """Wait for a started window and merge each query's GPU and CPU partial results."""
+        st["cpu_done"].wait()
+        st["read"].synchronize()
+        if st["cpu_err"]:
+            raise st["cpu_err"][0]
+        done_at = time.perf_counter()
+        hb = st["host"].numpy()
         results, off = [], 0
-        for q, hr in zip(queries, host_res):
+        split = len(st["csegs"]) > 0
+        for q, hr in zip(st["queries"], st["host_res"]):
             nb = 8 if q.template == "agg" else 16 * q.groups
             g = hb[off: off + nb].view(np.int32).copy()
             off += nb
-            results.append(merge(q, g, hr) if len(csegs) else g)
-        ms = (time.perf_counter() - t0) * 1e3
-        return WindowRun(results, ms, len(queries), len(segs), len(gsegs), len(csegs), staged, launches, span,
-                         plan_ms=plan_ms, gpu_ms=g0.elapsed_time(g1), cpu_ms=cpu_ms[0], copied_column_segments=copied,
-                         extra={"waves": waves})
+            results.append(merge(q, g, hr) if split else g)
+        return WindowRun(results, (done_at - st["t0"]) * 1e3, len(st["queries"]), len(st["segs"]),
+                         len(st["gsegs"]), len(st["csegs"]), st["staged"], st["launches"], st["span"],
+                         plan_ms=st["plan_ms"], gpu_ms=st["g0"].elapsed_time(st["g1"]), cpu_ms=st["cpu_ms"][0],
+                         copied_column_segments=st["copied"], extra={"waves": st["waves"], "done_at": done_at})
+
+    def run_window(self, queries: list[B.Query], planner) -> WindowRun:
+        """One window on its own: planned, run and merged before returning."""
+        return self._finish_window(self._start_window(queries, planner))
 
     def run(self, queries: list[B.Query], planner, window: int = 256) -> list[WindowRun]:
-        """All queries in windows of `window`, in order."""
-        return [self.run_window(queries[i: i + window], planner) for i in range(0, len(queries), window)]
+        """All queries in windows of `window`, in order. Window k + 1 is planned and
+        enqueued while window k's copies, scans and CPU share run (its scans queue behind
+        window k's on the kernel stream, its CPU share behind window k's on the CPU worker),
+        so the host-to-device link and the host cores do not idle between windows."""
+        runs, pending = [], None
+        for i in range(0, len(queries), window):
+            st = self._start_window(queries[i: i + window], planner)
+            if pending is not None:
+                runs.append(self._finish_window(pending))
+            pending = st
+        if pending is not None:
+            runs.append(self._finish_window(pending))
+        return runs

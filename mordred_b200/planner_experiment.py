@@ -174,7 +174,9 @@ def evaluate_batched(bx, planners: list, queries: list[B.Query], start_weights: 
         res = [r for w in runs for r in w.results]
         if keep_results is not None:
             keep_results[p.name] = res
-        done = np.cumsum([w.ms for w in runs])
+        # windows overlap (the next is planned and enqueued while one runs): a query
+        # completes when its window's results are merged
+        done = np.array([(w.extra["done_at"] - t0) * 1e3 for w in runs])
         per_query = np.repeat(done, [w.queries for w in runs])
         out[p.name] = {"total_ms": total, "windows": len(runs), "window_queries": window,
                        "mean_window_ms": float(np.mean([w.ms for w in runs])),
