@@ -52,14 +52,17 @@ struct __align__(16) AQ {
   int soff;                 // shared-memory byte offset of the 64-bit sums; < 0: sums by L2
                             // atomics, and soff <= -2 puts the keys' touch bitmap at -soff - 2
   int flags;                // bits 0-1 agg op, bit 2 CRYSTAL4 keys, bits 3-4 number of keys,
-                            // bits 8-16 queries in its family, bits 17-25 its place in it
+                            // bits 8-16 its family's group stride, bits 17-25 its place in it
 };
 // A family is a set of queries with the same group count whose shared-memory sums are
 // interleaved group-major: the sum of group g of the family's j-th query lies at
-// base + 8 * (g * members + j) (soff = base + 8 * j), so the matches of one row — same
+// base + 8 * (g * stride + j) (soff = base + 8 * j), so the matches of one row — same
 // group, neighbouring queries — hit neighbouring words rather than banks at random. The
-// members' touch bitmaps follow the sums: base + 8 * total * members + 4 * words * j.
-// A query alone is a family of one (the plain layout).
+// stride is the member count rounded up to an odd number: matches of one query to
+// different groups (rows of one date on a date-sorted table match the same queries) then
+// fall in different bank pairs, where an even stride that is a multiple of 16 would put
+// them all in one. The members' touch bitmaps follow the sums:
+// base + 8 * total * stride + 4 * words * j. A query alone is a family of one.
 __device__ __forceinline__ int aq_family(const AQ& A) { return (A.flags >> 8) & 0x1ff; }
 __device__ __forceinline__ int aq_member(const AQ& A) { return (A.flags >> 17) & 0x1ff; }
 static_assert(sizeof(AQ) == 32, "aggregation descriptor size");
@@ -992,7 +995,7 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
     }
     if (total == 0) break;
     const int words = (total + 31) / 32;
-    auto fam_bytes = [&](int k) { return (8 * total * k + 4 * words * k + 15) / 16 * 16; };
+    auto fam_bytes = [&](int k) { return (8 * total * (k | 1) + 4 * words * k + 15) / 16 * 16; };
     int members = 0;
     for (int qi = 0; qi < P.nq; ++qi) {
       const AQ& A = P.q[qi].a;
@@ -1008,7 +1011,7 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
       if (P.q[qi].res_layout == MB_RES_SCALAR || A.soff >= 0 || A.total != total) continue;
       if (j < members) {
         A.soff = off + groups_bytes + 8 * j;
-        A.flags = (A.flags & 0xff) | (members << 8) | (j << 17);
+        A.flags = (A.flags & 0xff) | ((members | 1) << 8) | (j << 17);
         ++j;
       } else {
         A.flags |= 1 << 30;  // no room: sums by L2 atomics (marked so the search moves on)

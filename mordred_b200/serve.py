@@ -171,7 +171,8 @@ class PlannerRouter:
     `spare_cores`); its results equal the GPU's (integer sums; rows outside the candidate
     segments cannot match the query's date range)."""
 
-    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0, spare_cores: int = 2):
+    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0, spare_cores: int = 2,
+                 max_segments: int = 24):
         from .engine import FACT, CpuShare, host_tables
 
         class _Share(CpuShare):
@@ -191,6 +192,9 @@ class PlannerRouter:
         self._predict = getattr(planner, "predict_host", planner.predict)
         self.margin = margin
         self.max_backlog_ms = max_backlog_ms
+        # the decision runs on the serving thread for every arrival: queries over more
+        # candidate segments than this are left to the GPU without consulting the model
+        self.max_segments = max_segments
         self.gpu_lat = collections.deque(maxlen=64)
         self.backlog_ms = 0.0
         self.q: queue.Queue = queue.Queue()
@@ -212,6 +216,8 @@ class PlannerRouter:
         if len(self.gpu_lat) < 8:
             return False  # no GPU latency seen yet
         cand = self.share.candidates(q)
+        if len(cand) > self.max_segments:
+            return False
         if len(cand) == 0:
             pred = 0.0
         else:

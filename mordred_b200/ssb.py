@@ -301,7 +301,7 @@ def star_args(**kw) -> L.MbStarArgs:
     for i, col in enumerate(aggr):
         a.aggr[i] = _p(col)
     for k, v in kw.items():
-        if k in ("res", "count", "gpu_cache", "segment_group"):
+        if k in ("res", "count", "gpu_cache", "segment_group", "rows"):
             v = _p(v)
         setattr(a, k, v)
     return a
