@@ -178,13 +178,25 @@ __device__ __forceinline__ AQ load_aq(const AQ* s_aq, int qi) {
   return a;
 }
 
+// The 32-bit value a match adds (sign-extended to 64 bits by the caller), as the
+// single-query path computes it: SUM a0, SUB a0 - a1, MUL a0 * a1 (wrapping).
+template <class Get>
+__device__ __forceinline__ unsigned batch_value(const AQ& A, Get get) {
+  const unsigned v0 = static_cast<unsigned>(get(A.a0)), v1 = static_cast<unsigned>(get(A.a1));
+  const int op = A.flags & 3;
+  return op == MB_AGG_SUM ? v0 : op == MB_AGG_SUB ? v0 - v1 : v0 * v1;
+}
+
+// A query whose sum is one shared-memory word (a scalar, or one group without keys).
+__device__ __forceinline__ bool aq_single_word(const AQ& A) {
+  return A.soff >= 0 && A.total == 1 && !((A.flags >> 2) & 1);
+}
+
 // Add one (row, query) match: `get(code)` reads a field of the row.
 template <class Get>
 __device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int qi, Get get, unsigned char* smem,
                                             bool& bad_group) {
-  const unsigned v0 = static_cast<unsigned>(get(A.a0)), v1 = static_cast<unsigned>(get(A.a1));
-  const int op = A.flags & 3;
-  const unsigned u = op == MB_AGG_SUM ? v0 : op == MB_AGG_SUB ? v0 - v1 : v0 * v1;
+  const unsigned u = batch_value(A, get);
   const unsigned long long w = static_cast<unsigned long long>(static_cast<long long>(static_cast<int>(u)));
   const int k0 = get(A.k0), k1 = get(A.k1);
   const unsigned hh = static_cast<unsigned>(k0) * A.kmul0 + static_cast<unsigned>(k1) * A.kmul1 + A.bias;
@@ -444,11 +456,27 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
       auto flush = [&](int n) {
         for (int base = 0; base < n; base += 32) {
           const int idx = base + lane;
-          if (idx < n) {
-            const unsigned pr = mlist[idx];
-            const int row = static_cast<int>(pr >> 16), qi = static_cast<int>(pr & 0xffffu);
-            auto get = [&](int code) { return field_value(wst[(code >> 11) * CS + row], code); };
-            batch_match(load_aq(s_aq, qi), s_res, qi, get, smem, bad_group);
+          const bool valid = idx < n;
+          const unsigned pr = valid ? mlist[idx] : 0u;
+          const int row = static_cast<int>(pr >> 16), qi = static_cast<int>(pr & 0xffffu);
+          auto get = [&](int code) { return field_value(wst[(code >> 11) * CS + row], code); };
+          AQ A{};
+          if (valid) A = load_aq(s_aq, qi);
+          const bool single = valid && aq_single_word(A);
+          const unsigned single_lanes = __ballot_sync(kFullMask, single);
+          if (single) {
+            // the lanes holding matches of one such query add across the warp first and
+            // one of them updates its word: rows of one date (a date-sorted table) match
+            // the same queries, and same-word shared-memory atomics serialise
+            const unsigned u = batch_value(A, get);
+            const unsigned peers = __match_any_sync(single_lanes, qi);
+            const unsigned lo = __reduce_add_sync(peers, u & 0xffffu);          // < 2^21 over 32 lanes
+            const int hi = __reduce_add_sync(peers, static_cast<int>(u) >> 16);  // |.| <= 2^20
+            if (lane == __ffs(peers) - 1)
+              atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff),
+                        static_cast<unsigned long long>(static_cast<long long>(hi) * 65536 + lo));
+          } else if (valid) {
+            batch_match(A, s_res, qi, get, smem, bad_group);
           }
         }
         __syncwarp();

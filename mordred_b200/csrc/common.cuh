@@ -13,6 +13,18 @@
 
 namespace mb {
 
+static __device__ __noinline__ int slow_mod(int d, int m) { return d % m; }
+
+// ((key - key_min) % slots) in 32-bit two's complement (crystal/join.cuh:3). Keys in
+// [key_min, key_min + slots) map to themselves and the next range wraps by one
+// subtraction (a dense 1-based key N lands on slot 0); only other keys divide.
+__device__ __forceinline__ int pht_slot(int key, int slots, int kmin) {
+  const int d = static_cast<int>(static_cast<unsigned>(key) - static_cast<unsigned>(kmin));
+  if (static_cast<unsigned>(d) < static_cast<unsigned>(slots)) return d;
+  if (static_cast<unsigned>(d) < 2u * static_cast<unsigned>(slots) && slots <= (1 << 30)) return d - slots;
+  return slow_mod(d, slots);
+}
+
 // Longest a CTA waits on one bulk-copy stage before it gives up, sets
 // MB_STATUS_TIMEOUT and returns (a healthy copy lands in microseconds).
 constexpr unsigned long long kWaitLimitNs = 4000000000ull;

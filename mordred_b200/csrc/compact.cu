@@ -84,9 +84,7 @@ __global__ void __launch_bounds__(256) select_kernel(const __grid_constant__ Sel
       int outv[MB_MAX_PROBES] = {0, 0, 0, 0};
       for (int p = 0; p < P.np; ++p) {
         if (!ok) break;
-        const int key = load(P.pkey[p]);
-        const int d = static_cast<int>(static_cast<unsigned>(key) - static_cast<unsigned>(P.pkmin[p]));
-        const int h = d % P.pslots[p];
+        const int h = pht_slot(load(P.pkey[p]), P.pslots[p], P.pkmin[p]);
         if (h < 0) {
           bad_probe = true;
           ok = false;

@@ -258,7 +258,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
 
   // ---- launch configuration and shared-memory plan ------------------------------
   // Unset fields take the tuned configuration for this query shape (tuned_configs.h).
-  const TunedConfig tc = tuned_config(P.nf, a->num_probes, a->probe[0].layout, P.res_layout, P.total_val);
+  const TunedConfig tc = tuned_config(P.nf, a->num_probes, a->probe[0].layout, P.res_layout, P.total_val, P.n);
   const int threads = a->threads ? a->threads : tc.threads;
   const int items = a->items_per_thread ? a->items_per_thread : tc.items;
   if (threads % 32 != 0 || threads < 128 || threads > 512) return MB_ERR_ARG;

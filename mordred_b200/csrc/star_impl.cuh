@@ -33,18 +33,6 @@ __device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
 
 // Out-of-line remainder for the rare keys outside [key_min, key_min + 2*slots): kept as
 // a call so the hot path never carries an if-converted division.
-static __device__ __noinline__ int slow_mod(int d, int m) { return d % m; }
-
-// ((key - key_min) % slots) in 32-bit two's complement (crystal/join.cuh:3). Keys in
-// [key_min, key_min + slots) map to themselves and the next range wraps by one
-// subtraction (a dense 1-based key N lands on slot 0); only other keys divide.
-__device__ __forceinline__ int pht_slot(int key, int slots, int kmin) {
-  const int d = static_cast<int>(static_cast<unsigned>(key) - static_cast<unsigned>(kmin));
-  if (static_cast<unsigned>(d) < static_cast<unsigned>(slots)) return d;
-  if (static_cast<unsigned>(d) < 2u * static_cast<unsigned>(slots) && slots <= (1 << 30)) return d - slots;
-  return slow_mod(d, slots);
-}
-
 __device__ __forceinline__ bool aligned16_dev(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {

@@ -2,7 +2,10 @@
 // shape, written by mordred_b200/autotune.py from sweeps on a B200 (threads x rows per
 // thread x stages x group mode, 120,000,000-row fact table). A shape is keyed by its
 // filter count, probe count, first probe's table layout, whether it groups, and whether
-// its group array is large (> 2,048 groups). Unknown shapes take kDefaultConfig.
+// its group array is large (> 2,048 groups); an entry with max_rows > 0 applies only to
+// calls of at most that many rows and is looked up first (small tables: 6,000,000 rows
+// swept over 20 separate tables replayed back to back from a CUDA graph). Unknown shapes
+// take kDefaultConfig.
 #pragma once
 
 namespace mb {
@@ -15,23 +18,27 @@ struct TunedConfig {
 struct TunedEntry {
   int nf, np, p0_layout, grouped, big_groups;
   TunedConfig cfg;
+  long long max_rows = 0;  // > 0: only for calls of at most this many rows
 };
 
 static const TunedConfig kDefaultConfig = {256, 8, 2, 0};
 
 static const TunedEntry kTuned[] = {
+    {3, 0, -1, 0, 0, {128, 16, 3, 0}, 16ll << 20},  // filter-aggregate, 6 M rows: 0.0185 ms, 5.19 TB/s
     {3, 0, -1, 0, 0, {256, 16, 4, 0}},  // filter-aggregate (q11 form): 0.268 ms, 7.16 TB/s
     {0, 3, 0, 1, 1, {256, 8, 2, 2}},  // Query A form: 0.452 ms, 4.25 TB/s
     {0, 4, 0, 1, 0, {512, 8, 4, 1}},  // Query B form: 0.708 ms, 4.07 TB/s
     {0, 4, 2, 1, 0, {256, 8, 2, 1}},  // engine four-table group-by: 0.876 ms, 3.29 TB/s
 };
 
-inline TunedConfig tuned_config(int nf, int np, int p0_layout, int res_layout, int total_val) {
+inline TunedConfig tuned_config(int nf, int np, int p0_layout, int res_layout, int total_val, long long rows) {
   const int grouped = res_layout != 0 ? 1 : 0;
   const int big = grouped && total_val > 2048 ? 1 : 0;
   const int l0 = np > 0 ? p0_layout : -1;
   for (const TunedEntry& e : kTuned)
-    if (e.nf == nf && e.np == np && e.p0_layout == l0 && e.grouped == grouped && e.big_groups == big) return e.cfg;
+    if (e.nf == nf && e.np == np && e.p0_layout == l0 && e.grouped == grouped && e.big_groups == big &&
+        (e.max_rows == 0 || rows <= e.max_rows))
+      return e.cfg;
   TunedConfig c = kDefaultConfig;
   if (big) c.group_mode = 2;  // large group arrays: L2 atomics keep shared memory for stages
   return c;

@@ -111,6 +111,7 @@ class ServeReport:
     peak_held_bytes: int = 0
     scan_rows: int = 0          # fact rows the launches scanned
     cpu_answered: int = 0       # queries the router sent to the host cores
+    cap_raises: int = 0         # circular scan: times the active-set cap rose under a backlog
 
     def summary(self, rows: int) -> dict:
         lat = sorted(self.latencies_ms)
@@ -123,7 +124,8 @@ class ServeReport:
                 "fact_rows_per_s": (self.scan_rows or self.batches * rows) / self.seconds if self.seconds else None,
                 "query_rows_per_s": len(lat) * rows / self.seconds if self.seconds else None,
                 "rejected": self.rejected, "deferred_admissions": self.deferred,
-                "peak_admitted_bytes": self.peak_held_bytes, "cpu_answered": self.cpu_answered}
+                "peak_admitted_bytes": self.peak_held_bytes, "cpu_answered": self.cpu_answered,
+                "cap_raises": self.cap_raises}
 
 
 def _drain_cpu(router, rep: ServeReport, results: dict, queries, arrivals, t0: float, keep: bool) -> int:
@@ -349,17 +351,22 @@ class CircularServer:
     those of the query run alone. Up to 256 queries share a launch; a second launch is
     queued before the first completes so the GPU never waits for the host."""
 
-    # At most 128 queries share a launch: a batch of up to 128 carries 4 words of query mask
-    # per attribute value, more than 128 carry 8, and every row's mask work doubles — under a
-    # burst that slows every launch of the lap the burst joins, which lets the active set grow
-    # further. Queries beyond the cap wait in arrival order for the next launch.
+    # Load-following cap on the active set. Up to 128 queries a launch carry 4 words of query
+    # mask per attribute value and more carry 8, which doubles every row's mask work; below
+    # saturation the scan therefore keeps at most `max_active` (128) queries, so that a burst
+    # cannot tip it into the slower 8-word launches. When admitted queries have waited longer
+    # than one lap for a place (the 128-query scan answers fewer queries per second than
+    # arrive), the cap rises to `burst_active` (256): a lap then costs more but answers twice
+    # the queries, so the backlog drains instead of growing without bound. The cap falls
+    # back once nothing waits and the active set is back within `max_active`.
     def __init__(self, t: dict, sizes: ssb.Sizes, n_rows: int, budget_bytes: int = 16 << 30,
-                 max_active: int = 128, chunks: int = 8):
+                 max_active: int = 128, chunks: int = 8, burst_active: int = L.MB_BATCH_MAX_QUERIES):
         self.t, self.sizes, self.n = t, sizes, n_rows
         self.pats = B.build_pats(t, sizes)
         self.dims = self.pats.c_dims()
         self.budget = budget_bytes
         self.max_active = max_active
+        self.burst_active = max(max_active, burst_active)
         step = -(-n_rows // max(1, chunks))
         step = -(-step // 4096) * 4096  # 16-byte aligned chunk starts
         self.bounds = [(r0, min(n_rows, r0 + step)) for r0 in range(0, n_rows, step)] or [(0, 0)]
@@ -398,6 +405,9 @@ class CircularServer:
         c = 0
         done = 0
         i = 0
+        cap = self.max_active
+        lap_s = None               # duration of the last full lap (s)
+        lap_start, lap_c = None, 0
         t0 = time.perf_counter()
         while done + ac.rejected < len(queries):
             now = time.perf_counter() - t0
@@ -405,7 +415,15 @@ class CircularServer:
                 _arrive(ac, router, i, queries[i], nbytes[i])
                 i += 1
             done += _drain_cpu(router, rep, results, queries, arrivals, t0, keep_results)
-            for qid, nb in ac.take(self.max_active - len(active)):
+            # the cap follows the load: raised while the oldest admitted query has waited
+            # for a place longer than a lap, lowered when the backlog is gone
+            if ac.admitted and lap_s is not None and cap < self.burst_active:
+                if now - arrivals[ac.admitted[0][0]] > lap_s:
+                    cap = self.burst_active
+                    rep.cap_raises += 1
+            elif not ac.admitted and cap > self.max_active and len(active) <= self.max_active:
+                cap = self.max_active
+            for qid, nb in ac.take(cap - len(active)):
                 res = queries[qid].result_buffer()
                 active.append(_Member(qid, nb, queries[qid], queries[qid].to_c(res), res))
             rep.peak_held_bytes = max(rep.peak_held_bytes, ac.held)
@@ -424,6 +442,12 @@ class CircularServer:
                 rep.batches += 1
                 rep.batch_sizes.append(len(members))
                 rep.scan_rows += self.bounds[c][1] - self.bounds[c][0]
+                if c == 0:
+                    tl = time.perf_counter()
+                    if lap_start is not None and lap_c == nchunks:
+                        lap_s = tl - lap_start
+                    lap_start, lap_c = tl, 0
+                lap_c += 1
                 c = (c + 1) % nchunks
                 continue
             if inflight:

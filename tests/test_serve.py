@@ -74,7 +74,7 @@ def test_circular_server_answers_every_query_exactly(chunks):
     n = 3_000_001
     sizes = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
     t = ssb.gen_device(sizes, 29, B.BATCH_FACT, B.BATCH_DIMS)
-    srv = S.CircularServer(t, sizes, n, budget_bytes=4 << 20, max_active=64, chunks=chunks)
+    srv = S.CircularServer(t, sizes, n, budget_bytes=4 << 20, max_active=64, chunks=chunks, burst_active=64)
     assert len(srv.bounds) == chunks and srv.bounds[-1][1] == n
     qs = B.generate_queries(300, seed=5, sel_lo=1e-4, sel_hi=0.3)
     arr = S.poisson_arrivals(3000.0, len(qs), 7)
@@ -85,6 +85,32 @@ def test_circular_server_answers_every_query_exactly(chunks):
     assert all(x > 0 for x in rep.latencies_ms)
     ws = B.AloneWorkspace(sizes)
     for qid in range(0, 300, 7):
+        r = qs[qid].result_buffer()
+        B.run_alone(t, ws, qs[qid], r, n)
+        assert np.array_equal(res[qid].reshape(-1), r.cpu().numpy().reshape(-1)), qid
+    assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
+def test_circular_server_raises_its_cap_under_a_backlog():
+    """A burst larger than the active-set cap: the cap rises to burst_active while admitted
+    queries wait longer than a lap, never beyond it, and every result stays exact."""
+    import torch
+    from mordred_b200 import _lib as L
+    from mordred_b200 import ssb
+    torch.cuda.set_device(0)
+    n = 2_000_003
+    sizes = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    t = ssb.gen_device(sizes, 31, B.BATCH_FACT, B.BATCH_DIMS)
+    srv = S.CircularServer(t, sizes, n, budget_bytes=64 << 20, max_active=8, chunks=4, burst_active=40)
+    qs = B.generate_queries(240, seed=11, sel_lo=1e-4, sel_hi=0.3)
+    # 40 queries at first, then the other 200 all at once after the first laps
+    arr = np.concatenate([np.linspace(0.0, 0.002, 40), np.full(200, 0.05)])
+    rep, res = srv.serve(qs, arr, keep_results=True)
+    assert rep.summary(n)["completed"] == 240
+    assert rep.cap_raises >= 1 and max(rep.batch_sizes) <= 40 and max(rep.batch_sizes) > 8
+    ws = B.AloneWorkspace(sizes)
+    for qid in range(0, 240, 11):
         r = qs[qid].result_buffer()
         B.run_alone(t, ws, qs[qid], r, n)
         assert np.array_equal(res[qid].reshape(-1), r.cpu().numpy().reshape(-1)), qid
