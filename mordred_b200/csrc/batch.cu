@@ -39,6 +39,9 @@ constexpr int kColPad = 4;                 // words between staged columns: the 
 constexpr int kMaxStageCols = MB_NUM_FACT_COLS + 1;
 constexpr int kMaxBreakpoints = 768;       // range end points of wide attributes, over all of them
 constexpr int kMaxBuckets = 2048;          // bucket index entries per wide attribute
+constexpr int kScalarCopies = 4;           // shared-memory copies of each scalar sum, one per lane mod 4:
+                                           // rows of one date (a date-sorted table) match the same
+                                           // scalar queries, and same-word atomics of one warp serialise
 
 // Field codes inside the kernel address staged columns: (stage column << 11) | (shift << 6) | width.
 // Aggregation descriptor of one query (32 bytes, shared memory). The group index is
@@ -52,7 +55,9 @@ struct __align__(16) AQ {
   int soff;                 // shared-memory byte offset of the 64-bit sums; < 0: sums by L2
                             // atomics, and soff <= -2 puts the keys' touch bitmap at -soff - 2
   int flags;                // bits 0-1 agg op, bit 2 CRYSTAL4 keys, bits 3-4 number of keys,
-                            // bits 8-16 its family's group stride, bits 17-25 its place in it
+                            // bit 5 a scalar kept in kScalarCopies words (lane mod 4 adds to
+                            // its own), bits 8-16 its family's group stride, bits 17-25 its
+                            // place in it
 };
 // A family is a set of queries with the same group count whose shared-memory sums are
 // interleaved group-major: the sum of group g of the family's j-th query lies at
@@ -110,6 +115,7 @@ struct BatchPlan {
   long long table_entries;
   int stages, stage_words, list_cap;
   int smem_acc_off, smem_aq_off, smem_res_off, smem_pres_off, smem_out_off, smem_list_off;
+  int acc_words;                   // 8-byte scalar words (kScalarCopies per scalar query)
   int smem_groups_off, smem_groups_words, smem_stage_off;
   unsigned int* status;
   // segment-cache addressing: col[c] is a per-segment slot array into gpu_cache
@@ -187,11 +193,6 @@ __device__ __forceinline__ unsigned batch_value(const AQ& A, Get get) {
   return op == MB_AGG_SUM ? v0 : op == MB_AGG_SUB ? v0 - v1 : v0 * v1;
 }
 
-// A query whose sum is one shared-memory word (a scalar, or one group without keys).
-__device__ __forceinline__ bool aq_single_word(const AQ& A) {
-  return A.soff >= 0 && A.total == 1 && !((A.flags >> 2) & 1);
-}
-
 // Add one (row, query) match: `get(code)` reads a field of the row.
 template <class Get>
 __device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int qi, Get get, unsigned char* smem,
@@ -211,7 +212,8 @@ __device__ __forceinline__ void batch_match(const AQ& A, void* const* s_res, int
   const bool c4 = (A.flags >> 2) & 1;
   if (A.soff >= 0) {
     const int fam = aq_family(A), j = aq_member(A);
-    atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff) + g * fam, w);
+    const int copy = (A.flags >> 5) & 1 ? static_cast<int>(threadIdx.x & (kScalarCopies - 1)) : 0;
+    atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff) + g * fam + copy, w);
     if (!c4) return;
     // the first row of a group in this CTA writes the group's keys
     uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + A.soff - 8 * j + 8 * A.total * fam) +
@@ -301,10 +303,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
   // ---- set-up: accumulators, descriptors, masks, small tables, barriers ------------
   {
     unsigned long long* s_acc = reinterpret_cast<unsigned long long*>(smem + P.smem_acc_off);
-    for (int q = tid; q < P.nq; q += NWARPS * 32) {
-      s_acc[q] = 0;
-      s_res[q] = P.q[q].res;
-    }
+    for (int w = tid; w < P.acc_words; w += NWARPS * 32) s_acc[w] = 0;
+    for (int q = tid; q < P.nq; q += NWARPS * 32) s_res[q] = P.q[q].res;
     unsigned* dst = reinterpret_cast<unsigned*>(s_aq);
     for (int w = tid; w < P.nq * 8; w += NWARPS * 32) dst[w] = reinterpret_cast<const unsigned*>(&P.q[w >> 3].a)[w & 7];
     for (int w = tid; w < 16 * kMaskWordsMax; w += NWARPS * 32) s_pres[w] = (&P.pres_mask[0][0])[w];
@@ -456,27 +456,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
       auto flush = [&](int n) {
         for (int base = 0; base < n; base += 32) {
           const int idx = base + lane;
-          const bool valid = idx < n;
-          const unsigned pr = valid ? mlist[idx] : 0u;
-          const int row = static_cast<int>(pr >> 16), qi = static_cast<int>(pr & 0xffffu);
-          auto get = [&](int code) { return field_value(wst[(code >> 11) * CS + row], code); };
-          AQ A{};
-          if (valid) A = load_aq(s_aq, qi);
-          const bool single = valid && aq_single_word(A);
-          const unsigned single_lanes = __ballot_sync(kFullMask, single);
-          if (single) {
-            // the lanes holding matches of one such query add across the warp first and
-            // one of them updates its word: rows of one date (a date-sorted table) match
-            // the same queries, and same-word shared-memory atomics serialise
-            const unsigned u = batch_value(A, get);
-            const unsigned peers = __match_any_sync(single_lanes, qi);
-            const unsigned lo = __reduce_add_sync(peers, u & 0xffffu);          // < 2^21 over 32 lanes
-            const int hi = __reduce_add_sync(peers, static_cast<int>(u) >> 16);  // |.| <= 2^20
-            if (lane == __ffs(peers) - 1)
-              atomicAdd(reinterpret_cast<unsigned long long*>(smem + A.soff),
-                        static_cast<unsigned long long>(static_cast<long long>(hi) * 65536 + lo));
-          } else if (valid) {
-            batch_match(A, s_res, qi, get, smem, bad_group);
+          if (idx < n) {
+            const unsigned pr = mlist[idx];
+            const int row = static_cast<int>(pr >> 16), qi = static_cast<int>(pr & 0xffffu);
+            auto get = [&](int code) { return field_value(wst[(code >> 11) * CS + row], code); };
+            batch_match(load_aq(s_aq, qi), s_res, qi, get, smem, bad_group);
           }
         }
         __syncwarp();
@@ -589,8 +573,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
     const unsigned long long* s_sum = reinterpret_cast<const unsigned long long*>(smem + A.soff);
     const bool c4 = (A.flags >> 2) & 1;
     const int fam = aq_family(A);
+    const bool copies = (A.flags >> 5) & 1;
     for (int g = tid; g < A.total; g += NWARPS * 32) {
-      const unsigned long long v = s_sum[g * fam];
+      unsigned long long v = s_sum[g * fam];
+      if (copies)
+        for (int k = 1; k < kScalarCopies; ++k) v += s_sum[k];
       if (v == 0) continue;
       atomicAdd(c4 ? reinterpret_cast<unsigned long long*>(static_cast<int*>(s_res[q]) + 4 * g + 2)
                    : static_cast<unsigned long long*>(s_res[q]) + g,
@@ -959,8 +946,11 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   // presence masks | outside masks | small predicate tables | match lists |
   // small group arrays | stage ring
   int off = 2 * kBatchStages * 8;
+  int nscalar = 0;
+  for (int qi = 0; qi < P.nq; ++qi) nscalar += P.q[qi].res_layout == MB_RES_SCALAR ? 1 : 0;
   P.smem_acc_off = off;
-  off += 8 * P.nq;
+  P.acc_words = kScalarCopies * nscalar;
+  off += 8 * P.acc_words;
   off = (off + 15) / 16 * 16;
   P.smem_aq_off = off;
   off += static_cast<int>(sizeof(AQ)) * P.nq;
@@ -996,9 +986,12 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   while (total_smem(off, stages) > budget && stages > 2) --stages;
   if (total_smem(off, stages) > budget) return MB_ERR_SIZE;
   P.stages = stages;
-  // scalars accumulate in their shared-memory word
-  for (int qi = 0; qi < P.nq; ++qi)
-    if (P.q[qi].res_layout == MB_RES_SCALAR) P.q[qi].a.soff = P.smem_acc_off + 8 * qi;
+  // scalars accumulate in their shared-memory words (kScalarCopies each)
+  for (int qi = 0, k = 0; qi < P.nq; ++qi)
+    if (P.q[qi].res_layout == MB_RES_SCALAR) {
+      P.q[qi].a.soff = P.smem_acc_off + 8 * kScalarCopies * k++;
+      P.q[qi].a.flags |= 1 << 5;
+    }
   // small group arrays (<= 1,024 groups) to shared memory, smallest first, within the budget
   P.smem_groups_off = off;
   int groups_bytes = 0;

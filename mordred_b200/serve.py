@@ -169,11 +169,11 @@ class PlannerRouter:
     skipping on the date-sorted table) plus the CPU queue's predicted backlog, against
     `margin` x the GPU latency the server has been seeing (a running median of recent GPU
     completions). The CPU side is one worker thread running queries one at a time on the
-    CPU engine (mb_cpu_star_query over the pinned host columns, all host threads but
-    `spare_cores`); its results equal the GPU's (integer sums; rows outside the candidate
+    CPU engine (mb_cpu_star_query over the pinned host columns, on `cpu_share` of the host
+    threads); its results equal the GPU's (integer sums; rows outside the candidate
     segments cannot match the query's date range)."""
 
-    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0, spare_cores: int = 2,
+    def __init__(self, table, planner, margin: float = 0.5, max_backlog_ms: float = 50.0, cpu_share: float = 0.5,
                  max_segments: int = 24):
         from .engine import FACT, CpuShare, host_tables
 
@@ -185,9 +185,10 @@ class PlannerRouter:
         self.share.hht = host_tables(table.sizes)
         self.share.cache = _AllResident(table.nseg, len(FACT))
         from . import cpu as _cpu
-        # the serving thread (planning, launches, result copies) keeps `spare_cores` cores:
-        # a CPU engine on every core slows the GPU path it is meant to relieve
-        self.share.cpu_nthreads = max(1, _cpu.threads() - spare_cores)
+        # the serving thread (planning, launches, result copies) keeps the other threads: a
+        # CPU engine on every core slows the GPU path it is meant to relieve (measured: GPU
+        # batches took longer and latency rose with all host threads routed)
+        self.share.cpu_nthreads = max(1, int(_cpu.threads() * cpu_share))
         self.share.cpu_threads = self.share.cpu_nthreads
         self.planner = planner
         # predictions on the host: a forward launch would queue behind the batch kernels
