@@ -414,10 +414,12 @@ def serve_section(args, table=None):
     date-sorted table of --serve-rows rows, a 16 GB admission budget, the batched kernel.
     Two GPU servers — whole-scan batches (up to 256 queries a launch) and the circular scan
     (admitted queries join the running scan at the next of 8 chunks and complete after one
-    lap, at most 128 at a time) — each with the learned planner routing the queries it
-    predicts the host cores answer sooner to the CPU engine; over three arrival seeds, and
-    once without the router for comparison. Latency: arrival to completion. Results are
-    checked against the queries run alone for a sample."""
+    lap; at most 128 at a time, 256 while a backlog waits longer than a lap) — each with
+    the learned planner's router, which sheds queries the host cores answer sooner to the
+    CPU engine once the GPU misses its latency target; over three arrival seeds, once
+    without the router, and once at 1.4x the rate (circular scan, router on and off).
+    Latency: arrival to completion. Results are checked against the queries run alone for
+    a sample."""
     import numpy as np
     import torch
 
@@ -473,6 +475,20 @@ def serve_section(args, table=None):
         rep, _ = srv.serve(qs, arrivals)
         summ = rep.summary(table.n)
         no_router[name] = {kk: summ[kk] for kk in keys}
+    # overload: 1.4x the rate on the circular scan, with the router shedding load to the
+    # host cores and without it
+    stress_rate = 1.4 * args.serve_rate
+    n2 = int(stress_rate * args.serve_seconds)
+    qs2 = B.generate_queries(n2, seed=SEED + 7)
+    arr2 = S.poisson_arrivals(stress_rate, n2, SEED + 9)
+    stress = {"rate_qps": stress_rate}
+    for label, use in (("router", True), ("no_router", False)):
+        router = S.PlannerRouter(table, planner) if use and planner is not None else None
+        rep, _ = circ.serve(qs2, arr2, router=router)
+        if router is not None:
+            router.close()
+        summ = rep.summary(table.n)
+        stress[label] = {kk: summ[kk] for kk in keys + ("cap_raises",)}
     del whole, circ, t
     torch.cuda.empty_cache()
     p99 = lambda name: [r["p99_ms"] for r in runs[name]]
@@ -481,7 +497,7 @@ def serve_section(args, table=None):
             "selectivity": "log-uniform in [1e-5, 0.3]", "seeds": 3, "router": "learned planner" if planner else None,
             "whole_scan_batches": runs["whole"], "circular_scan_8_chunks_max_128_active": runs["circular"],
             "p99_ms_whole_by_seed": p99("whole"), "p99_ms_circular_by_seed": p99("circular"),
-            "without_router_first_seed": no_router, "routing": routing,
+            "without_router_first_seed": no_router, "overload_circular": stress, "routing": routing,
             "results_checked_against_alone": checked,
             "qps": runs["circular"][0]["qps"], "p50_ms": runs["circular"][0]["p50_ms"],
             "p99_ms": max(p99("circular"))}
