@@ -32,6 +32,7 @@ import ctypes as C
 import math
 import queue
 import statistics
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -214,6 +215,11 @@ class PlannerRouter:
         self.pred_ms: list[float] = []
         self.cpu_ms: list[float] = []
         self._lock = threading.Lock()
+        # the serving thread has to get the interpreter back within a fraction of one launch
+        # (a few ms) whenever the worker runs Python between its engine calls; the default
+        # 5 ms switch interval can hand the worker a whole launch's worth of time
+        self._switch = sys.getswitchinterval()
+        sys.setswitchinterval(min(self._switch, 2e-4))
         self._th = threading.Thread(target=self._worker, daemon=True)
         self._th.start()
 
@@ -265,6 +271,7 @@ class PlannerRouter:
     def close(self) -> None:
         self.q.put(None)
         self._th.join(timeout=60)
+        sys.setswitchinterval(self._switch)
 
     def summary(self) -> dict:
         err = [abs(math.log(max(p, 1e-3)) - math.log(max(m, 1e-3))) for p, m in zip(self.pred_ms, self.cpu_ms)]
@@ -348,18 +355,26 @@ class _Member:
     query: B.Query
     cq: L.MbBatchQuery          # the query's launch descriptor, made once at admission
     res: torch.Tensor           # its device result, accumulated over the chunks
-    launched: int = 0           # chunks launched for it so far
+    pending: np.ndarray = None  # per chunk: still to be launched for it (bool)
+    left: int = 0               # chunks still to be launched for it
 
 
 class CircularServer:
     """Cooperative circular scan: the GPU-resident table is split into `chunks` row
     ranges that one batched launch after another visits in a cycle. An admitted query
-    joins the running scan at the next launch and completes once every chunk has been
-    launched for it (one full lap from wherever it joined), so it waits for about one
-    scan of the table rather than for the batch in progress plus its own. Every query
-    sees every row exactly once and the kernel only adds into its result, so results are
-    those of the query run alone. Up to 256 queries share a launch; a second launch is
-    queued before the first completes so the GPU never waits for the host."""
+    joins the running scan at the next launch and completes once every chunk it needs has
+    been launched for it (within one lap from wherever it joined), so it waits for about
+    one scan of the table rather than for the batch in progress plus its own. Every query
+    sees every row it needs exactly once and the kernel only adds into its result, so
+    results are those of the query run alone. Up to 256 queries share a launch; a second
+    launch is queued before the first completes so the GPU never waits for the host.
+
+    Chunk skipping (`skip`, the planner's segment skipping, QueryOptimizer.cu:1641-1662):
+    each chunk's orderdate [min, max] is taken when the server starts; a query needs only
+    the chunks whose range meets its date range (rows elsewhere cannot pass its date
+    predicate), and the scan moves on to the next chunk some active query needs, so on a
+    date-sorted table a query over a few weeks costs one chunk's launch, not a lap, and
+    chunks no active query needs are not scanned at all."""
 
     # Load-following cap on the active set. Up to 128 queries a launch carry 4 words of query
     # mask per attribute value and more carry 8, which doubles every row's mask work; below
@@ -370,7 +385,8 @@ class CircularServer:
     # the queries, so the backlog drains instead of growing without bound. The cap falls
     # back once nothing waits and the active set is back within `max_active`.
     def __init__(self, t: dict, sizes: ssb.Sizes, n_rows: int, budget_bytes: int = 16 << 30,
-                 max_active: int = 128, chunks: int = 8, burst_active: int = L.MB_BATCH_MAX_QUERIES):
+                 max_active: int = 128, chunks: int = 8, burst_active: int = L.MB_BATCH_MAX_QUERIES,
+                 skip: bool = True):
         self.t, self.sizes, self.n = t, sizes, n_rows
         self.pats = B.build_pats(t, sizes)
         self.dims = self.pats.c_dims()
@@ -381,6 +397,17 @@ class CircularServer:
         step = -(-step // 4096) * 4096  # 16-byte aligned chunk starts
         self.bounds = [(r0, min(n_rows, r0 + step)) for r0 in range(0, n_rows, step)] or [(0, 0)]
         self.ws = torch.empty(16, dtype=torch.uint8, device=next(iter(t.values())).device)
+        self.skip = skip
+        od = t["lo_orderdate"]
+        rng = [torch.aminmax(od[r0:r1]) if r1 > r0 else (torch.tensor(1), torch.tensor(0)) for r0, r1 in self.bounds]
+        self.chunk_lo = np.array([int(lo) for lo, _ in rng], np.int64)
+        self.chunk_hi = np.array([int(hi) for _, hi in rng], np.int64)
+
+    def chunks_needed(self, q: B.Query) -> np.ndarray:
+        """Per chunk, whether q can have a matching row in it (all chunks without skipping)."""
+        if not self.skip:
+            return np.ones(len(self.bounds), bool)
+        return (self.chunk_hi >= q.date[0]) & (self.chunk_lo <= q.date[1])
 
     def _launch(self, c: int, members: list) -> None:
         r0, r1 = self.bounds[c]
@@ -411,13 +438,14 @@ class CircularServer:
         nbytes = [query_bytes(q) for q in queries]
         nchunks = len(self.bounds)
         active: list[_Member] = []            # still have chunks to be launched
+        instant: list[_Member] = []           # need no chunk: complete at admission
         inflight: collections.deque = collections.deque()  # (event, members finishing with it, launch time)
         c = 0
         done = 0
         i = 0
         cap = self.max_active
-        lap_s = None               # duration of the last full lap (s)
-        lap_start, lap_c = None, 0
+        lap_s = None               # duration of the last lap of the scan position (s)
+        lap_start = None
         t0 = time.perf_counter()
         while done + ac.rejected < len(queries):
             now = time.perf_counter() - t0
@@ -435,29 +463,48 @@ class CircularServer:
                 cap = self.max_active
             for qid, nb in ac.take(cap - len(active)):
                 res = queries[qid].result_buffer()
-                active.append(_Member(qid, nb, queries[qid], queries[qid].to_c(res), res))
+                need = self.chunks_needed(queries[qid])
+                m = _Member(qid, nb, queries[qid], queries[qid].to_c(res), res, need.copy(), int(need.sum()))
+                (active if m.left else instant).append(m)
+            if instant:
+                # no chunk can hold a matching row: the (zeroed) result is the answer
+                end = time.perf_counter() - t0
+                for m in instant:
+                    if keep_results:
+                        results[m.qid] = m.res.cpu().numpy().reshape(-1).view(
+                            np.int64 if m.query.template == "agg" else np.int32).copy()
+                    rep.latencies_ms.append((end - arrivals[m.qid]) * 1e3)
+                    ac.release(m.nbytes)
+                done += len(instant)
+                instant = []
             rep.peak_held_bytes = max(rep.peak_held_bytes, ac.held)
             if active and len(inflight) < 2:
-                members = list(active)
+                # the next chunk (cyclically from the scan position) some active query needs
+                want = np.zeros(nchunks, bool)
+                for m in active:
+                    want |= m.pending
+                step = int(np.argmax(np.roll(want, -c)))
+                if c + step >= nchunks or lap_start is None:  # the scan wraps: a lap ends
+                    tl = time.perf_counter()
+                    if lap_start is not None:
+                        lap_s = tl - lap_start
+                    lap_start = tl
+                c = (c + step) % nchunks
+                members = [m for m in active if m.pending[c]]
                 self._launch(c, members)
                 ev = torch.cuda.Event()
                 ev.record()
                 finishing = []
                 for m in members:
-                    m.launched += 1
-                    if m.launched == nchunks:
+                    m.pending[c] = False
+                    m.left -= 1
+                    if m.left == 0:
                         finishing.append(m)
-                active = [m for m in active if m.launched < nchunks]
+                active = [m for m in active if m.left > 0]
                 inflight.append((ev, finishing, time.perf_counter()))
                 rep.batches += 1
                 rep.batch_sizes.append(len(members))
                 rep.scan_rows += self.bounds[c][1] - self.bounds[c][0]
-                if c == 0:
-                    tl = time.perf_counter()
-                    if lap_start is not None and lap_c == nchunks:
-                        lap_s = tl - lap_start
-                    lap_start, lap_c = tl, 0
-                lap_c += 1
                 c = (c + 1) % nchunks
                 continue
             if inflight:

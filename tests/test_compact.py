@@ -40,18 +40,21 @@ def _qb_probes(s, t, ws):
 
 
 def _expected(s, t, ws, date):
-    """(rows, nation payloads) passing the date filter and Query B's four probes (numpy)."""
-    h = {k: v.cpu().numpy().astype(np.int64) for k, v in t.items()}
-    hs, hc, hp, hd = (ws[k].cpu().numpy() for k in ("ht_s", "ht_c", "ht_p_b", "ht_d"))
-    ok = (h["lo_orderdate"] >= date[0]) & (h["lo_orderdate"] <= date[1])
-    ok &= hs[h["lo_suppkey"] % s.s_len] != 0
-    cs = h["lo_custkey"] % s.c_len
-    ok &= (hc[2 * cs] != 0) | (hc[2 * cs + 1] != 0)
-    ok &= hp[h["lo_partkey"] % s.p_len] != 0
-    ds = h["lo_orderdate"] - ssb.DATE_MIN
-    ok &= (hd[2 * ds] != 0) | (hd[2 * ds + 1] != 0)
-    rows = np.nonzero(ok)[0]
-    return rows, hc[2 * cs + 1][rows]
+    """(rows, probe outputs) passing the date filter and Query B's four probes: the
+    oracle's selection (orc_select) over the same columns and tables, in row order."""
+    from oracle import oracle as O
+    h = {k: v.cpu().numpy() for k, v in t.items()}
+    hw = {k: ws[k].cpu().numpy() for k in ("ht_s", "ht_c", "ht_p_b", "ht_d")}
+    probes = [dict(fkey=h["lo_suppkey"], ht=hw["ht_s"], num_slots=s.s_len, layout=L.MB_HT_KEY),
+              dict(fkey=h["lo_custkey"], ht=hw["ht_c"], num_slots=s.c_len, layout=L.MB_HT_KEY_VAL),
+              dict(fkey=h["lo_partkey"], ht=hw["ht_p_b"], num_slots=s.p_len, layout=L.MB_HT_KEY),
+              dict(fkey=h["lo_orderdate"], ht=hw["ht_d"], num_slots=ssb.DATE_SLOTS, key_min=ssb.DATE_MIN,
+                   layout=L.MB_HT_KEY_VAL)]
+    rows, dims, k, st = O.select(len(h["lo_orderdate"]),
+                                 filters=[dict(col=h["lo_orderdate"], mode=L.MB_FILTER_BETWEEN, c1=date[0],
+                                               c2=date[1])], probes=probes)
+    assert st == 0 and k == len(rows)
+    return rows, dims
 
 
 def test_select_offset_list_and_payloads():
@@ -66,12 +69,13 @@ def test_select_offset_list_and_payloads():
     total = torch.zeros(1, dtype=torch.int32, device="cuda")
     L.call("mb_star_select", C.byref(args), None, 0, lo.data_ptr(), dptr, n, total.data_ptr(), ssb._stream())
     k = int(total.item())
-    rows, nations = _expected(s, t, ws, date)
+    rows, odims = _expected(s, t, ws, date)
     assert k == len(rows) > 0
     order = torch.argsort(lo[:k]).cpu().numpy()
     got_rows = lo[:k].cpu().numpy()[order]
     assert np.array_equal(got_rows, rows)
-    assert np.array_equal(dim[1][:k].cpu().numpy()[order], nations)   # customer payload = nation
+    for j in range(4):                                                 # payloads: none, nation, none, year
+        assert np.array_equal(dim[j][:k].cpu().numpy()[order], odims[j]), j
     assert (dim[0][:k] == 0).all()                                     # KEY layout: no payload
     years = dim[3][:k].cpu().numpy()[order]
     assert years.min() >= 1994 and years.max() <= 1996

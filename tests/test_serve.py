@@ -92,6 +92,39 @@ def test_circular_server_answers_every_query_exactly(chunks):
 
 
 @pytest.mark.gpu
+def test_circular_server_skips_chunks_outside_a_query_dates():
+    """Over a date-sorted table a query joins only the chunks whose orderdate range meets
+    its own; queries needing one chunk, several, or none all get their results alone."""
+    import dataclasses
+
+    import torch
+    from mordred_b200 import _lib as L
+    from mordred_b200 import ssb
+    from mordred_b200.engine import SegmentedTable
+    torch.cuda.set_device(0)
+    n = 6 * (1 << 20) + 777
+    sizes = ssb.Sizes(lo_len=n, s_len=4_000, c_len=60_000, p_len=100_000)
+    table = SegmentedTable(n, 37, sizes)
+    t = {k: torch.from_numpy(table.host[k]).cuda() for k in B.BATCH_FACT}
+    t.update(table.dims)
+    t.update(ssb.gen_device(sizes, 37, [], [d for d in B.BATCH_DIMS if d not in t]))
+    srv = S.CircularServer(t, sizes, n, budget_bytes=64 << 20, max_active=64, chunks=8)
+    qs = B.generate_queries(150, seed=21, sel_lo=1e-4, sel_hi=0.3)
+    qs += [dataclasses.replace(q, date=(19990101, 19991231)) for q in qs[:5]]  # no row can match
+    need = [int(srv.chunks_needed(q).sum()) for q in qs]
+    assert min(need) == 0 and any(0 < k < 8 for k in need) and max(need) == 8
+    arr = S.poisson_arrivals(2000.0, len(qs), 23)
+    rep, res = srv.serve(qs, arr, keep_results=True)
+    assert rep.summary(n)["completed"] == len(qs)
+    ws = B.AloneWorkspace(sizes)
+    for qid in range(len(qs)):
+        r = qs[qid].result_buffer()
+        B.run_alone(t, ws, qs[qid], r, n)
+        assert np.array_equal(np.asarray(res[qid]).reshape(-1).view(np.int32), r.cpu().numpy().reshape(-1).view(np.int32)), qid
+    assert L.device_status(0) == 0
+
+
+@pytest.mark.gpu
 def test_circular_server_raises_its_cap_under_a_backlog():
     """A burst larger than the active-set cap: the cap rises to burst_active while admitted
     queries wait longer than a lap, never beyond it, and every result stays exact."""
