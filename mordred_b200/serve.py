@@ -445,7 +445,7 @@ class CircularServer:
         i = 0
         cap = self.max_active
         lap_s = None               # duration of the last lap of the scan position (s)
-        lap_start = None
+        lap_start, last_c = None, -1
         t0 = time.perf_counter()
         while done + ac.rejected < len(queries):
             now = time.perf_counter() - t0
@@ -484,12 +484,13 @@ class CircularServer:
                 for m in active:
                     want |= m.pending
                 step = int(np.argmax(np.roll(want, -c)))
-                if c + step >= nchunks or lap_start is None:  # the scan wraps: a lap ends
+                c = (c + step) % nchunks
+                if lap_start is None or c <= last_c:  # the scan position wrapped: a lap ends
                     tl = time.perf_counter()
                     if lap_start is not None:
                         lap_s = tl - lap_start
                     lap_start = tl
-                c = (c + step) % nchunks
+                last_c = c
                 members = [m for m in active if m.pending[c]]
                 self._launch(c, members)
                 ev = torch.cuda.Event()
