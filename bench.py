@@ -489,12 +489,13 @@ def serve_section(args, table=None):
             router.close()
         summ = rep.summary(table.n)
         stress[label] = {kk: summ[kk] for kk in keys + ("cap_raises",)}
+    skipping = circ.skip
     del whole, circ, t
     torch.cuda.empty_cache()
     p99 = lambda name: [r["p99_ms"] for r in runs[name]]
     return {"rows": table.n, "rate_qps": args.serve_rate, "seconds_per_run": args.serve_seconds,
             "budget_bytes": 16 << 30, "table": "date-sorted, GPU-resident (9 fact columns)",
-            "circular_chunk_skipping": circ.skip,
+            "circular_chunk_skipping": skipping,
             "selectivity": "log-uniform in [1e-5, 0.3]", "seeds": 3, "router": "learned planner" if planner else None,
             "whole_scan_batches": runs["whole"], "circular_scan_8_chunks_max_128_active": runs["circular"],
             "p99_ms_whole_by_seed": p99("whole"), "p99_ms_circular_by_seed": p99("circular"),
