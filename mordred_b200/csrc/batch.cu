@@ -256,7 +256,6 @@ __device__ __forceinline__ void batch_row_mask(const BatchPlan& P, unsigned pres
     if (NWM == 1 && m[0] == 0) return;
     const int v = get(P.f_scode[f]) - P.f_min[f];
     const unsigned* t;
-    int sw = 0;  // the half-swap of the shared-memory layout (8-word entries)
     if (static_cast<unsigned>(v) < static_cast<unsigned>(P.f_n[f])) {
       int e = v;
       if (P.f_nint[f] > 0) {
@@ -264,18 +263,14 @@ __device__ __forceinline__ void batch_row_mask(const BatchPlan& P, unsigned pres
         e = reinterpret_cast<const uint16_t*>(smem + P.f_bkt_off[f])[v >> P.f_shift[f]];
         while (e + 1 < P.f_nint[f] && bp[e + 1] <= v) ++e;
       }
-      if (P.f_smem_off[f] >= 0) {
-        t = reinterpret_cast<const unsigned*>(smem + P.f_smem_off[f]) + e * P.nwords;
-        if (NWM == 8) sw = ((e >> 2) & 1) << 2;
-      } else {
-        t = P.tables + P.f_goff[f] + static_cast<long long>(e) * P.nwords;
-      }
+      t = P.f_smem_off[f] >= 0 ? reinterpret_cast<const unsigned*>(smem + P.f_smem_off[f]) + e * P.nwords
+                               : P.tables + P.f_goff[f] + static_cast<long long>(e) * P.nwords;
     } else
       t = s_out + f * kMaskWordsMax;
     if (NWM >= 4) {
 #pragma unroll
       for (int w = 0; w < NWM; w += 4) {
-        const uint4 u = *reinterpret_cast<const uint4*>(t + (w ^ sw));
+        const uint4 u = *reinterpret_cast<const uint4*>(t + w);
         m[w] &= u.x;
         m[w + 1] &= u.y;
         m[w + 2] &= u.z;
@@ -320,10 +315,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
       if (P.f_smem_off[f] < 0) continue;
       unsigned* t = reinterpret_cast<unsigned*>(smem + P.f_smem_off[f]);
       const unsigned* s = P.tables + P.f_goff[f];
-      // 8-word entries: the two 16-byte halves of entries 4..7 (mod 8) trade places, so the
-      // first halves of eight consecutive entries cover all eight 16-byte bank groups
-      for (int w = tid; w < P.f_ent[f] * P.nwords; w += NWARPS * 32)
-        t[P.nwords == 8 ? w ^ (((w >> 5) & 1) << 2) : w] = s[w];
+      for (int w = tid; w < P.f_ent[f] * P.nwords; w += NWARPS * 32) t[w] = s[w];
       if (P.f_nint[f] > 0) {
         int* bp = reinterpret_cast<int*>(smem + P.f_bps_off[f]);
         for (int i = tid; i < P.f_nint[f]; i += NWARPS * 32) bp[i] = P.bp[P.f_bp_off[f] + i];
