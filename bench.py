@@ -388,6 +388,7 @@ def planner_section(args, table=None):
     bx = BatchExecutor(table, cache_slots=slots)
     batched = PE.evaluate_batched(bx, [AnalyticPlanner(), learned], queries, start, log=lambda *a: None,
                                   keep_results=batch_res)
+    bx.close()
     bx.cache.close()
     del bx
     torch.cuda.empty_cache()

@@ -223,6 +223,18 @@ class BatchExecutor(CpuShare):
         self._stage_buf = buf
         return launches, len(waves), staged
 
+    def close(self) -> None:
+        """Stop the CPU worker (after the windows already handed to it)."""
+        if self._cpu_worker.is_alive():
+            self._cpu_jobs.put(None)
+            self._cpu_worker.join(timeout=60)
+
+    def __enter__(self) -> "BatchExecutor":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
     # ---- one window ---------------------------------------------------------------------------
     def _cpu_loop(self) -> None:
         """The windows' CPU shares, one after another (they share the host hash tables)."""

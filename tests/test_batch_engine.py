@@ -70,6 +70,7 @@ def test_windows_equal_oracle_and_one_at_a_time(table):
         if planner.name == "cpu":
             assert sum(w.gpu_segments for w in runs) == 0
     # the one-query-at-a-time executor agrees
+    ex.close()
     one = Executor(table, cache_slots=40)
     for i, q in enumerate(qs[:20]):
         assert np.array_equal(one.run(q, AnalyticPlanner()).result, exp[i])
@@ -84,5 +85,6 @@ def test_admission_keeps_demanded_segments_resident(table):
     # every window reads the first two months only: those segments become resident
     qs = [dataclasses.replace(q, date=(19920105, 19920225)) for q in B.generate_queries(30, seed=9)]
     runs = ex.run(qs, AnalyticPlanner(), window=10)
+    ex.close()
     assert runs[0].copied_column_segments > 0
     assert all(w.staged_segments == 0 for w in runs[1:])

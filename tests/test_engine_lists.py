@@ -299,6 +299,33 @@ def test_star_query_rows_generic_direct_columns():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("k", [0, 1, 31, 33, 100_003])
+def test_star_query_rows_edge_sizes_and_large_group_array(k):
+    """Offset lists of 0, 1 and around one warp of entries, and a list form whose group
+    array (12,000 groups, engine layout) is too large for shared memory, against the
+    oracle."""
+    import torch
+    rng = np.random.default_rng(k + 1)
+    n = 300_007
+    key = rng.integers(1, 50_001, n).astype(np.int32)
+    val = rng.integers(-1000, 1_000_000, n).astype(np.int32)
+    dk = np.arange(1, 50_001, dtype=np.int32)
+    ht = np.zeros(2 * 50_000, np.int32)
+    O.build_ht((dk % 4).astype(np.int32), 1, 0, 2, dk, (dk * 7 % 12_000).astype(np.int32), ht, 50_000, 0, 1)
+    rows = rng.choice(n, k, replace=False).astype(np.int32)
+    res = torch.zeros(6 * 12_000, dtype=torch.int32, device="cuda")
+    probes = lambda kk, hh: [dict(fkey=kk, ht=hh, num_slots=50_000, layout=1, unique_val=1, res_slot=2)]
+    a = ssb.star_args(num_rows=k, probes=probes(_dev(key), _dev(ht)), aggr=[_dev(val)], agg_op=L.MB_AGG_SUM,
+                      total_val=12_000, res_layout=L.MB_RES_ENGINE6, res=res, rows=_dev(rows))
+    ssb.star_query(a)
+    exp = np.zeros(6 * 12_000, np.int32)
+    O.star(k, rows=rows, probes=probes(key, ht), aggr=[val], agg_op=0, total_val=12_000, res_layout=1, res=exp)
+    assert np.array_equal(res.cpu().numpy(), exp)
+    assert exp.any() if k >= 31 else True
+    assert L.device_status(0, clear=True) == 0
+
+
+@pytest.mark.gpu
 def test_list_builds_and_minmax():
     """build_GPU3 and build_GPU_minmax2 over a list of dimension rows, build_GPU_minmax over a
     segment range, against the oracle (tables and key ranges)."""
