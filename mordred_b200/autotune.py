@@ -192,13 +192,20 @@ def tune_small(n: int = 6_000_000, copies: int = 20, reps: int = 10, verbose: bo
             "rows": n, "max_rows": 16 << 20, "best": best, "gbs": gbs, "runs": runs}
 
 
+# Shapes whose sparse phase runs the packed second round (star_kernel<..., PACK = true>):
+# measured at 120 M rows, it pays for the Query B shape (0.685 against 0.711 ms) and costs
+# the Query A (0.565 against 0.460) and engine shapes (1.03 against 0.87).
+PACKED_SHAPES = {(0, 4, 0, 1, 0)}
+
+
 def write(results: list[dict], gpu: str) -> None:
     lines = []
     for r in sorted(results, key=lambda r: -r.get("max_rows", 0)):  # row-limited entries first
         b, k = r["best"], r["key"]
         limit = f", {r['max_rows'] >> 20}ll << 20" if r.get("max_rows") else ""
+        pack = ", 0, 1" if tuple(k) in PACKED_SHAPES else ""
         lines.append(f"    {{{k[0]}, {k[1]}, {k[2]}, {k[3]}, {k[4]}, {{{b['threads']}, {b['items']}, {b['stages']}, "
-                     f"{b['group_mode']}}}{limit}}},  // {r['shape']}: {b['ms']:.4f} ms, {r['gbs'] / 1000:.2f} TB/s")
+                     f"{b['group_mode']}{pack}}}{limit}}},  // {r['shape']}: {b['ms']:.4f} ms, {r['gbs'] / 1000:.2f} TB/s")
     text = open(HEADER).read()
     head, rest = text.split("static const TunedEntry kTuned[] = {\n", 1)
     _, tail = rest.split("};\n", 1)

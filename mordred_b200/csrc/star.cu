@@ -23,14 +23,15 @@ const Variant* star_variants_generic(int* count) {
 
 // The specialised variant for this shape if one was compiled, else the generic one. The
 // mirror-reading variants exist for specialised shapes only.
-static const Variant* find_variant(int warps, int items, int nf, int nd, int ns, bool mir) {
+static const Variant* find_variant(int warps, int items, int nf, int nd, int ns, bool mir, bool pack = false) {
   int n = 0;
   const Variant* sp = star_variants_special(&n);
   for (int i = 0; i < n; ++i)
     if (sp[i].warps == warps && sp[i].items == items && sp[i].nf == nf && sp[i].nd == nd && sp[i].ns == ns &&
-        sp[i].mir == mir)
+        sp[i].mir == mir && sp[i].pack == pack)
       return &sp[i];
   if (mir) return nullptr;
+  if (pack) return find_variant(warps, items, nf, nd, ns, false, false);  // no packing variant: plain one
   const Variant* g = star_variants_generic(&n);
   for (int i = 0; i < n; ++i)
     if (g[i].warps == warps && g[i].items == items) return &g[i];
@@ -315,7 +316,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   }
   if (smem > budget) smem = layout_smem(P, ncw, items, 2, false);
   if (smem > budget) return MB_ERR_SIZE;
-  if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false);
+  if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, tc.pack != 0);
   if (var == nullptr) return MB_ERR_ARG;
 
   long long want = P.nfull > 0 ? P.nfull : (P.n + threads - 1) / threads;

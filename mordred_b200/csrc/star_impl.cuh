@@ -22,7 +22,8 @@ using KernelFn = void (*)(StarPlan);
 struct Variant {
   int warps, items, nf, nd, ns;
   KernelFn fn;
-  bool mir = false;  // reads cluster-resident mirrors (launched with a cluster)
+  bool mir = false;   // reads cluster-resident mirrors (launched with a cluster)
+  bool pack = false;  // packs the first sparse probe's survivors across the warp
 };
 
 __device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
@@ -247,87 +248,160 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
   }
 }
 
-// Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes. The first
-// probe's loads go out alone, then the loads of every later probe together for the rows
-// the first kept; presence is combined probe by probe in order, so selection, payloads
-// and status bits equal the sequential chain.
+// One round of table probes: probes p0 + q for q in [qlo, qhi) (and q < nsp) for the rows
+// in `sel`. Every probe's loads go out before any is checked; presence is then combined
+// probe by probe in order, so selection, payloads (gv[q]) and status bits equal the
+// sequential chain.
+template <int ITEMS, class L>
+__device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint32_t& sel, int p0, int nsp, int qlo,
+                                            int qhi, int (&gv)[MB_MAX_PROBES][ITEMS], Accum& A,
+                                            const unsigned char* smem) {
+  int v[ITEMS];
+  unsigned long long sv[MB_MAX_PROBES][ITEMS];
+  uint32_t range_bad[MB_MAX_PROBES], absent[MB_MAX_PROBES];
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    range_bad[q] = 0;
+    absent[q] = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) sv[q][i] = 0;
+  }
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= nsp) break;
+    if (q < qlo || q >= qhi) continue;
+    const int p = p0 + q;
+    ld.load(P.p_col[p], v);
+    const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
+    const int* ht = P.p_ht[p];
+    const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      if (sel & (1u << i)) {
+        const int h = pht_slot(v[i], slots, kmin);
+        if (h < 0)
+          range_bad[q] |= 1u << i;
+        else if (bm != nullptr && !((bm[h >> 5] >> (h & 31)) & 1u))
+          absent[q] |= 1u << i;
+        else if (layout == MB_HT_KEY)
+          sv[q][i] = bm != nullptr ? 1ull : static_cast<unsigned long long>(static_cast<unsigned>(__ldg(ht + h)));
+        else
+          sv[q][i] = ldg_u64(ht + 2 * h);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= nsp) break;
+    if (q < qlo || q >= qhi) continue;
+    const int layout = P.p_layout[p0 + q];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      if (!(sel & (1u << i))) continue;
+      if (range_bad[q] & (1u << i)) {
+        A.bad_probe = true;
+        sel &= ~(1u << i);
+      } else if ((absent[q] & (1u << i)) || sv[q][i] == 0) {
+        sel &= ~(1u << i);
+      } else {
+        gv[q][i] = layout == MB_HT_KEY_VAL   ? static_cast<int>(sv[q][i] >> 32)
+                   : layout == MB_HT_VAL_OFF ? static_cast<int>(static_cast<unsigned>(sv[q][i]))
+                                             : 0;
+      }
+    }
+  }
+}
+
+// Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes, in two
+// rounds: the first table probe alone, then the others together for the rows it kept
+// (the first probe removes most rows, so later tables see a fraction of the loads, at
+// the price of one more L2 round trip). Per lane: usable from divergent code.
 template <int NSC, class L>
 __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint32_t sel, int p0, int ns,
                                             unsigned bias, Accum& A, unsigned long long* s_sum, uint32_t* s_touch,
                                             const unsigned char* smem) {
   constexpr int ITEMS = L::ITEMS;
   if (sel == 0) return;
-  int v[ITEMS];
   int gv[MB_MAX_PROBES][ITEMS];
-  unsigned long long sv[MB_MAX_PROBES][ITEMS];
-  uint32_t range_bad[MB_MAX_PROBES], absent[MB_MAX_PROBES];
 #pragma unroll
-  for (int p = 0; p < MB_MAX_PROBES; ++p) {
-    range_bad[p] = 0;
-    absent[p] = 0;
+  for (int q = 0; q < MB_MAX_PROBES; ++q)
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      gv[p][i] = 0;
-      sv[p][i] = 0;
-    }
-  }
-  // two rounds: the first table probe alone, then the others together for the rows it
-  // kept (the first probe removes most rows, so later tables see a fraction of the loads,
-  // at the price of one more L2 round trip)
+    for (int i = 0; i < ITEMS; ++i) gv[q][i] = 0;
   const int nsp = NSC >= 0 ? NSC : ns;
-#pragma unroll
-  for (int round = 0; round < 2; ++round) {
-    const int qlo = round == 0 ? 0 : 1, qhi = round == 0 ? 1 : MB_MAX_PROBES;
-#pragma unroll
-    for (int q = 0; q < MB_MAX_PROBES; ++q) {
-      if (q >= nsp) break;
-      if (q < qlo || q >= qhi) continue;
-      const int p = p0 + q;
-      ld.load(P.p_col[p], v);
-      const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
-      const int* ht = P.p_ht[p];
-      const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
-#pragma unroll
-      for (int i = 0; i < ITEMS; ++i) {
-        if (sel & (1u << i)) {
-          const int h = pht_slot(v[i], slots, kmin);
-          if (h < 0)
-            range_bad[q] |= 1u << i;
-          else if (bm != nullptr && !((bm[h >> 5] >> (h & 31)) & 1u))
-            absent[q] |= 1u << i;
-          else if (layout == MB_HT_KEY)
-            sv[q][i] = bm != nullptr ? 1ull : static_cast<unsigned long long>(static_cast<unsigned>(__ldg(ht + h)));
-          else
-            sv[q][i] = ldg_u64(ht + 2 * h);
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < MB_MAX_PROBES; ++q) {
-      if (q >= nsp) break;
-      if (q < qlo || q >= qhi) continue;
-      const int p = p0 + q;
-      const int layout = P.p_layout[p];
-#pragma unroll
-      for (int i = 0; i < ITEMS; ++i) {
-        if (!(sel & (1u << i))) continue;
-        if (range_bad[q] & (1u << i)) {
-          A.bad_probe = true;
-          sel &= ~(1u << i);
-        } else if ((absent[q] & (1u << i)) || sv[q][i] == 0) {
-          sel &= ~(1u << i);
-        } else {
-          gv[q][i] = layout == MB_HT_KEY_VAL   ? static_cast<int>(sv[q][i] >> 32)
-                     : layout == MB_HT_VAL_OFF ? static_cast<int>(static_cast<unsigned>(sv[q][i]))
-                                               : 0;
-        }
-      }
-    }
-    if (sel == 0) return;  // per lane; nothing warp-wide follows
-  }
+  probe_round<ITEMS>(P, ld, sel, p0, nsp, 0, 1, gv, A, smem);
+  if (sel == 0) return;
+  probe_round<ITEMS>(P, ld, sel, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
   if (P.count_after < 0) A.cnt += __popc(sel);
   if (sel == 0) return;
   aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
+}
+
+// Lane of the (k+1)-th set bit of `mask` (k < popc(mask)).
+__device__ __forceinline__ int nth_set_lane(uint32_t mask, int k) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1)
+    if (__popc(mask & ((2u << (lo + step - 1)) - 1u)) <= k) lo += step;
+  return lo;
+}
+
+// sparse_rows for a warp's batch of R survivors a lane, with the warp converged (every
+// lane calls it): after the first probe the rows it kept — about one in five — are packed
+// across the warp, one a lane (row offset and first payload moved by shuffles), so the
+// second round and the aggregate run once over full lanes instead of R times over mostly
+// empty ones.
+template <int NSC, int TILE, int R>
+__device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const GatherLoader<TILE, R>& ld, uint32_t sel,
+                                                   int p0, int ns, unsigned bias, Accum& A,
+                                                   unsigned long long* s_sum, uint32_t* s_touch,
+                                                   const unsigned char* smem) {
+  const int nsp = NSC >= 0 ? NSC : ns;
+  if (nsp < 2) {  // no second round to pack for
+    sparse_rows<NSC>(P, ld, sel, p0, ns, bias, A, s_sum, s_touch, smem);
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  int gv0[MB_MAX_PROBES][R];
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q)
+#pragma unroll
+    for (int i = 0; i < R; ++i) gv0[q][i] = 0;
+  probe_round<R>(P, ld, sel, p0, nsp, 0, 1, gv0, A, smem);
+  uint32_t b[R];
+  int c[R], total = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    b[i] = __ballot_sync(kFull, (sel >> i) & 1u);
+    c[i] = __popc(b[i]);
+    total += c[i];
+  }
+  // survivors in item-major order: every lane's item 0, then every lane's item 1, ...
+  for (int base = 0; base < total; base += 32) {
+    int rem = base + lane, row = 0, g = 0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const bool mine = rem >= 0 && rem < c[i];
+      const int src = mine ? nth_set_lane(b[i], rem) : lane;
+      const int xr = __shfl_sync(kFull, ld.r[i], src);
+      const int xg = __shfl_sync(kFull, gv0[0][i], src);
+      if (mine) {
+        row = xr;
+        g = xg;
+      }
+      rem -= c[i];
+    }
+    GatherLoader<TILE, 1> l1;
+    l1.wstage = ld.wstage;
+    l1.r[0] = row;
+    uint32_t s1 = base + lane < total ? 1u : 0u;
+    int gv[MB_MAX_PROBES][1];
+#pragma unroll
+    for (int q = 0; q < MB_MAX_PROBES; ++q) gv[q][0] = 0;
+    gv[0][0] = g;
+    probe_round<1>(P, l1, s1, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
+    if (P.count_after < 0) A.cnt += s1;
+    if (s1) aggregate_rows<NSC, 1>(P, l1, s1, gv, p0, ns, bias, A, s_sum, s_touch);
+  }
 }
 
 // The sparse phase with cluster-resident mirrors: a probe with a mirror tests presence —
@@ -548,7 +622,7 @@ __device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& 
   sparse_rows<-1>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
 }
 
-template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false>
+template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false, bool PACK = false>
 __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_constant__ StarPlan P) {
   constexpr int WROWS = 32 * ITEMS;
   constexpr int TILE = NCW * WROWS;
@@ -730,6 +804,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
         }
         if (MIR)
           sparse_rows_mir<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+        else if (PACK)
+          sparse_rows_packed<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
         else
           sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
       }

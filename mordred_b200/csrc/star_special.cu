@@ -9,6 +9,13 @@ namespace mb {
   {4, 16, NF, ND, NS, star_kernel<4, 16, NF, ND, NS>}, {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS>}, \
       {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS>}, {8, 16, NF, ND, NS, star_kernel<8, 16, NF, ND, NS>}
 
+// the same shapes packing the first sparse probe's survivors across the warp before the
+// second round (used where the tuned configuration asks for it)
+#define MB_PACK_VARIANTS(NF, ND, NS)                                                                \
+  {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS, false, true>, false, true},                      \
+      {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS, false, true>, false, true},                \
+      {8, 16, NF, ND, NS, star_kernel<8, 16, NF, ND, NS, false, true>, false, true}
+
 // the same shapes reading cluster-resident mirrors in the sparse phase
 #define MB_MIRROR_VARIANTS(NF, ND, NS)                                                        \
   {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS, true>, true},                              \
@@ -22,6 +29,7 @@ static const Variant kSpecial[] = {
     MB_SHAPE_VARIANTS(2, 1, 4),  // engine filter_probe_group_by: supplier bitmap, four tables
     MB_SHAPE_VARIANTS(0, 1, 4),  // engine probe_group_by: supplier bitmap, four tables
     MB_SHAPE_VARIANTS(0, 0, 1),  // src/ops probe, one table
+    MB_PACK_VARIANTS(0, 1, 3),
     MB_MIRROR_VARIANTS(0, 1, 2),
     MB_MIRROR_VARIANTS(0, 1, 3),
     MB_MIRROR_VARIANTS(2, 1, 4),
