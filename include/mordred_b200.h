@@ -143,6 +143,11 @@ typedef struct mb_star_args {
    * probes read on-chip memory instead of L2): 0 = the tuned default for the shape (large
    * calls only), 1 = never, 2 = whenever the tables fit. Results are the same either way. */
   int mirrors;
+  /* Second sparse round packed across the warp (the rows the first selective table probe
+   * kept are moved one a lane before the later probes and the aggregate run): 0 = the
+   * tuned default for the shape, 1 = never, 2 = where the shape has a packed variant.
+   * Results are the same either way. */
+  int pack;
 } mb_star_args;
 
 /* Fused filter -> chained probe -> group-by/aggregate over the fact table.

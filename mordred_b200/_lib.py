@@ -55,7 +55,8 @@ class MbStarArgs(C.Structure):
                 ("segment_group", C.c_void_p), ("start_offset", C.c_int64),
                 ("segment_size", C.c_int), ("threads", C.c_int),
                 ("items_per_thread", C.c_int), ("stages", C.c_int), ("grid", C.c_int),
-                ("group_mode", C.c_int), ("rows", C.c_void_p), ("mirrors", C.c_int)]
+                ("group_mode", C.c_int), ("rows", C.c_void_p), ("mirrors", C.c_int),
+                ("pack", C.c_int)]
 
 
 class MbFilterArgsGPU(C.Structure):

@@ -283,6 +283,8 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   if (group_mode == 1 && P.gmode != kGroupSmem) return MB_ERR_SIZE;
 
   if (a->mirrors < 0 || a->mirrors > 2) return MB_ERR_ARG;
+  if (a->pack < 0 || a->pack > 2) return MB_ERR_ARG;
+  const bool want_pack = a->pack == 2 || (a->pack == 0 && tc.pack != 0);
   const int budget = ds->max_smem_optin - 2048 - 2 * 8 * (ncw + 1);
   const int want_stages = a->stages ? a->stages : tc.stages;
   if (want_stages < 2 || want_stages > kMaxStages) return MB_ERR_ARG;
@@ -316,7 +318,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   }
   if (smem > budget) smem = layout_smem(P, ncw, items, 2, false);
   if (smem > budget) return MB_ERR_SIZE;
-  if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, tc.pack != 0);
+  if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, want_pack);
   if (var == nullptr) return MB_ERR_ARG;
 
   long long want = P.nfull > 0 ? P.nfull : (P.n + threads - 1) / threads;

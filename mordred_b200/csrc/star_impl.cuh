@@ -248,13 +248,13 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
   }
 }
 
-// One round of table probes: probes p0 + q for q in [qlo, qhi) (and q < nsp) for the rows
-// in `sel`. Every probe's loads go out before any is checked; presence is then combined
-// probe by probe in order, so selection, payloads (gv[q]) and status bits equal the
-// sequential chain.
+// One round of table probes: probes p0 + q for the q set in `qmask` (and q < nsp) for the
+// rows in `sel`. Every probe's loads go out before any is checked; presence is then
+// combined probe by probe in order, so selection, payloads (gv[q]) and status bits equal
+// the sequential chain.
 template <int ITEMS, class L>
-__device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint32_t& sel, int p0, int nsp, int qlo,
-                                            int qhi, int (&gv)[MB_MAX_PROBES][ITEMS], Accum& A,
+__device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint32_t& sel, int p0, int nsp,
+                                            uint32_t qmask, int (&gv)[MB_MAX_PROBES][ITEMS], Accum& A,
                                             const unsigned char* smem) {
   int v[ITEMS];
   unsigned long long sv[MB_MAX_PROBES][ITEMS];
@@ -269,7 +269,7 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
 #pragma unroll
   for (int q = 0; q < MB_MAX_PROBES; ++q) {
     if (q >= nsp) break;
-    if (q < qlo || q >= qhi) continue;
+    if (!((qmask >> q) & 1u)) continue;
     const int p = p0 + q;
     ld.load(P.p_col[p], v);
     const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
@@ -293,7 +293,7 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
 #pragma unroll
   for (int q = 0; q < MB_MAX_PROBES; ++q) {
     if (q >= nsp) break;
-    if (q < qlo || q >= qhi) continue;
+    if (!((qmask >> q) & 1u)) continue;
     const int layout = P.p_layout[p0 + q];
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
@@ -313,13 +313,15 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
 }
 
 // Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes, in two
-// rounds: the first table probe alone, then the others together for the rows it kept
-// (the first probe removes most rows, so later tables see a fraction of the loads, at
-// the price of one more L2 round trip). Per lane: usable from divergent code.
+// rounds: the first selective table probe alone (probe qf: the probes before it were
+// settled by their bitmaps in the dense phase and are only read for their payloads),
+// then the others together for the rows it kept (the first probe removes most rows, so
+// later tables see a fraction of the loads, at the price of one more L2 round trip). Per
+// lane: usable from divergent code.
 template <int NSC, class L>
 __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint32_t sel, int p0, int ns,
                                             unsigned bias, Accum& A, unsigned long long* s_sum, uint32_t* s_touch,
-                                            const unsigned char* smem) {
+                                            const unsigned char* smem, int qf = 0) {
   constexpr int ITEMS = L::ITEMS;
   if (sel == 0) return;
   int gv[MB_MAX_PROBES][ITEMS];
@@ -328,9 +330,10 @@ __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) gv[q][i] = 0;
   const int nsp = NSC >= 0 ? NSC : ns;
-  probe_round<ITEMS>(P, ld, sel, p0, nsp, 0, 1, gv, A, smem);
+  const uint32_t first = 1u << qf;
+  probe_round<ITEMS>(P, ld, sel, p0, nsp, first, gv, A, smem);
   if (sel == 0) return;
-  probe_round<ITEMS>(P, ld, sel, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
+  probe_round<ITEMS>(P, ld, sel, p0, nsp, ~first, gv, A, smem);
   if (P.count_after < 0) A.cnt += __popc(sel);
   if (sel == 0) return;
   aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
@@ -354,10 +357,10 @@ template <int NSC, int TILE, int R>
 __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const GatherLoader<TILE, R>& ld, uint32_t sel,
                                                    int p0, int ns, unsigned bias, Accum& A,
                                                    unsigned long long* s_sum, uint32_t* s_touch,
-                                                   const unsigned char* smem) {
+                                                   const unsigned char* smem, int qf) {
   const int nsp = NSC >= 0 ? NSC : ns;
   if (nsp < 2) {  // no second round to pack for
-    sparse_rows<NSC>(P, ld, sel, p0, ns, bias, A, s_sum, s_touch, smem);
+    sparse_rows<NSC>(P, ld, sel, p0, ns, bias, A, s_sum, s_touch, smem, qf);
     return;
   }
   const int lane = threadIdx.x & 31;
@@ -366,7 +369,8 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
   for (int q = 0; q < MB_MAX_PROBES; ++q)
 #pragma unroll
     for (int i = 0; i < R; ++i) gv0[q][i] = 0;
-  probe_round<R>(P, ld, sel, p0, nsp, 0, 1, gv0, A, smem);
+  const uint32_t first = 1u << qf;
+  probe_round<R>(P, ld, sel, p0, nsp, first, gv0, A, smem);
   uint32_t b[R];
   int c[R], total = 0;
 #pragma unroll
@@ -383,7 +387,7 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
       const bool mine = rem >= 0 && rem < c[i];
       const int src = mine ? nth_set_lane(b[i], rem) : lane;
       const int xr = __shfl_sync(kFull, ld.r[i], src);
-      const int xg = __shfl_sync(kFull, gv0[0][i], src);
+      const int xg = __shfl_sync(kFull, gv0[qf][i], src);
       if (mine) {
         row = xr;
         g = xg;
@@ -397,8 +401,8 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
     int gv[MB_MAX_PROBES][1];
 #pragma unroll
     for (int q = 0; q < MB_MAX_PROBES; ++q) gv[q][0] = 0;
-    gv[0][0] = g;
-    probe_round<1>(P, l1, s1, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
+    gv[qf][0] = g;
+    probe_round<1>(P, l1, s1, p0, nsp, ~first, gv, A, smem);
     if (P.count_after < 0) A.cnt += s1;
     if (s1) aggregate_rows<NSC, 1>(P, l1, s1, gv, p0, ns, bias, A, s_sum, s_touch);
   }
@@ -774,6 +778,9 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     uint16_t* list = reinterpret_cast<uint16_t*>(smem + P.smem_list_off) + cw * WROWS;
     const int nd = P.sparse_p0;  // the sparse phase starts at probe sparse_p0 <= n_dense
     const int ns = NSC >= 0 ? NSC : P.np - P.sparse_p0;
+    // the first sparse probe that can drop rows: those before it (p < n_dense) were
+    // tested against their bitmaps in the dense phase and are read only for payloads
+    const int qf = P.n_dense - P.sparse_p0 < ns ? P.n_dense - P.sparse_p0 : 0;
     const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
     if (MIR) {
       // this CTA's share of the mirrors, visible cluster-wide after the barrier
@@ -805,9 +812,9 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
         if (MIR)
           sparse_rows_mir<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
         else if (PACK)
-          sparse_rows_packed<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+          sparse_rows_packed<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, qf);
         else
-          sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+          sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, qf);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);

@@ -30,6 +30,8 @@ static const Variant kSpecial[] = {
     MB_SHAPE_VARIANTS(0, 1, 4),  // engine probe_group_by: supplier bitmap, four tables
     MB_SHAPE_VARIANTS(0, 0, 1),  // src/ops probe, one table
     MB_PACK_VARIANTS(0, 1, 3),
+    MB_PACK_VARIANTS(2, 1, 4),
+    MB_PACK_VARIANTS(0, 1, 4),
     MB_MIRROR_VARIANTS(0, 1, 2),
     MB_MIRROR_VARIANTS(0, 1, 3),
     MB_MIRROR_VARIANTS(2, 1, 4),

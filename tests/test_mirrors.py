@@ -26,7 +26,7 @@ def device():
 
 def _tables(n, seed, s_len=40_000, c_len=600_000, p_len=1_000_000):
     s = ssb.Sizes(lo_len=n, s_len=s_len, c_len=c_len, p_len=p_len)
-    t = ssb.gen_device(s, seed, ssb.QB_FACT, sorted(set(ssb.QA_DIMS + ssb.QB_DIMS)))
+    t = ssb.gen_device(s, seed, ssb.QB_FACT, sorted(set(ssb.QA_DIMS + ssb.QB_DIMS + ["s_nation"])))
     return s, t, {k: v.cpu().numpy() for k, v in t.items()}
 
 
@@ -155,4 +155,48 @@ def test_engine_four_table_shape_with_mirrors(cache):
         got = _run(probes(cols, 1), cols, n, [cols["lo_revenue"], cols["lo_supplycost"]], L.MB_AGG_SUB, 175,
                    L.MB_RES_ENGINE6, mirrors, 256, 8, **extra)
         assert np.array_equal(got, exp), (mirrors, cache)
+    assert L.device_status(0, clear=True) == 0
+
+
+@pytest.mark.parametrize("threads,items", [(256, 8), (512, 8), (256, 16)])
+def test_packed_second_round_query_b_and_engine_shapes(threads, items):
+    """The packed second sparse round (mb_star_args.pack = 2) and the plain one (1) equal
+    the oracle for the Query B shape (customer first) and the engine shape (supplier
+    settled by its bitmap and read for its payload after the customer probe)."""
+    n = 5_000_017
+    s, t, h = _tables(n, 91, s_len=20_000, c_len=300_000, p_len=500_000)
+    ht = {}
+    for name, flt, mode, c1, c2, key, val, slots, kmin, lay in [
+            ("s", "s_region", 0, 1, 0, "s_suppkey", None, s.s_len, 0, 0),
+            ("c", "c_region", 0, 1, 0, "c_custkey", "c_nation", s.c_len, 0, 1),
+            ("p", "p_mfgr", 2, 0, 1, "p_partkey", None, s.p_len, 0, 0),
+            ("d", None, 0, 0, 0, "d_datekey", "d_year", ssb.DATE_SLOTS, ssb.DATE_MIN, 1),
+            ("s2", "s_region", 1, 0, 2, "s_suppkey", "s_nation", s.s_len, 0, 2),
+            ("c2", "c_region", 0, 3, 0, "c_custkey", "c_nation", s.c_len, 0, 2),
+            ("p2", "p_mfgr", 2, 1, 4, "p_partkey", None, s.p_len, 0, 2),
+            ("d2", None, 0, 0, 0, "d_datekey", "d_year", ssb.DATE_SLOTS, ssb.DATE_MIN, 2)]:
+        a = np.zeros(2 * slots if lay else slots, np.int32)
+        O.build_ht(h[flt] if flt else None, mode, c1, c2, h[key], h[val] if val else None, a, slots, kmin, lay)
+        ht[name] = (a, _dev(a))
+    qb = lambda d, k: [dict(fkey=d["lo_suppkey"], ht=ht["s"][k], num_slots=s.s_len, layout=0),
+                       dict(fkey=d["lo_custkey"], ht=ht["c"][k], num_slots=s.c_len, layout=1, unique_val=7,
+                            res_slot=1),
+                       dict(fkey=d["lo_partkey"], ht=ht["p"][k], num_slots=s.p_len, layout=0),
+                       dict(fkey=d["lo_orderdate"], ht=ht["d"][k], num_slots=ssb.DATE_SLOTS, key_min=ssb.DATE_MIN,
+                            layout=1, min_val=1992, unique_val=1, res_slot=0)]
+    eng = lambda d, k: [dict(fkey=d["lo_suppkey"], ht=ht["s2"][k], num_slots=s.s_len, layout=2, unique_val=175,
+                             res_slot=0),
+                        dict(fkey=d["lo_custkey"], ht=ht["c2"][k], num_slots=s.c_len, layout=2, unique_val=7,
+                             res_slot=1),
+                        dict(fkey=d["lo_partkey"], ht=ht["p2"][k], num_slots=s.p_len, layout=2),
+                        dict(fkey=d["lo_orderdate"], ht=ht["d2"][k], num_slots=ssb.DATE_SLOTS, key_min=ssb.DATE_MIN,
+                             layout=2, min_val=1992, unique_val=1, res_slot=3)]
+    for probes, layout, total in ((qb, 2, 175), (eng, 1, 25 * 175)):
+        exp = np.zeros((4 if layout == 2 else 6) * total, np.int32)
+        assert O.star(n, probes=probes(h, 0), aggr=[h["lo_revenue"], h["lo_supplycost"]], agg_op=1, total_val=total,
+                      res_layout=layout, res=exp) == 0
+        for pack in (1, 2):
+            got = _run(probes(t, 1), t, n, [t["lo_revenue"], t["lo_supplycost"]], L.MB_AGG_SUB, total, layout, 1,
+                       threads, items, pack=pack)
+            assert np.array_equal(got, exp), (layout, pack, threads, items)
     assert L.device_status(0, clear=True) == 0
