@@ -321,6 +321,22 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, want_pack);
   if (var == nullptr) return MB_ERR_ARG;
 
+  // sparse visiting order of the tiled path: chain order, except that the first probe
+  // the dense phase did not settle goes first (a settled probe is present for every row
+  // the dense phase passes, so reading its payload later changes no result or status
+  // bit). The mirror-reading sparse phase and a payload-multiplied aggregate (which reads
+  // the first probe's payload) keep chain order.
+  const int ns_total = P.np - P.sparse_p0;
+  for (int q = 0; q < ns_total; ++q) P.sp_ord[q] = P.sparse_p0 + q;
+  if (!var->mir && P.agg_op != MB_AGG_MUL_PAYLOAD) {
+    const int first = P.n_dense - P.sparse_p0;
+    if (first > 0 && first < ns_total) {
+      const int lead = P.sp_ord[first];
+      for (int q = first; q > 0; --q) P.sp_ord[q] = P.sp_ord[q - 1];
+      P.sp_ord[0] = lead;
+    }
+  }
+
   long long want = P.nfull > 0 ? P.nfull : (P.n + threads - 1) / threads;
   if (want < 1) want = 1;
   if (var->mir) {

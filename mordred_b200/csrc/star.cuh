@@ -55,6 +55,9 @@ struct StarPlan {
                                   // probes whose payload is not needed stop before it, the
                                   // others are probed again there for their payload
   unsigned dense_bias;            // group terms (0 - min_val) * unique_val of probes < sparse_p0
+  int sp_ord[MB_MAX_PROBES];      // tiled path: probe visited at sparse position q (the first
+                                  // probe that can drop rows leads; the dense phase settled the
+                                  // probes it passes, which are read only for their payloads)
   int p_col[MB_MAX_PROBES];
   const int* p_ht[MB_MAX_PROBES];
   int p_slots[MB_MAX_PROBES], p_kmin[MB_MAX_PROBES], p_layout[MB_MAX_PROBES];

@@ -164,10 +164,19 @@ struct RowLoader {
   __device__ __forceinline__ void load(int c, int (&v)[1]) const { v[0] = __ldg(row_ptr(*P, c, r)); }
 };
 
-// Key columns of group h from the payloads of table probes p0.. (gv[q] = probe p0 + q).
-// Bitmap-decided probes have payload 0 and the caller zeroed the result, so they are
-// not written.
-template <int NSC, int ITEMS>
+// Probe index of sparse position q. The tiled path visits its sparse probes in the
+// planned order P.sp_ord (the first probe that can drop rows first, ahead of probes the
+// dense phase already settled and that are read only for their payloads); rows read
+// without a dense phase (the remainder) visit them in chain order from p0.
+template <bool ORD>
+__device__ __forceinline__ int sparse_probe(const StarPlan& P, int p0, int q) {
+  return ORD ? P.sp_ord[q] : p0 + q;
+}
+
+// Key columns of group h from the payloads of the sparse table probes (gv[q] = sparse
+// position q). Bitmap-decided probes have payload 0 and the caller zeroed the result, so
+// they are not written.
+template <int NSC, int ITEMS, bool ORD>
 __device__ __forceinline__ void write_keys(const StarPlan& P, int h, const int (&gv)[MB_MAX_PROBES][ITEMS], int i,
                                            int p0, int ns) {
   int* res = static_cast<int*>(P.res);
@@ -175,7 +184,7 @@ __device__ __forceinline__ void write_keys(const StarPlan& P, int h, const int (
 #pragma unroll
   for (int q = 0; q < MB_MAX_PROBES; ++q) {
     if (q >= (NSC >= 0 ? NSC : ns)) break;
-    const int rs = P.p_res_slot[p0 + q];
+    const int rs = P.p_res_slot[sparse_probe<ORD>(P, p0, q)];
     if (rs >= 0) res[stride * h + rs] = gv[q][i];
   }
 }
@@ -196,7 +205,7 @@ struct Accum {
 // Aggregate the rows still selected in `sel` into the scalar or the groups. gv[q] is the
 // payload of table probe p0 + q; `bias` already holds the group terms of every probe
 // before p0 (bitmap-decided probes, payload 0).
-template <int NSC, int ITEMS, class L>
+template <int NSC, int ITEMS, bool ORD, class L>
 __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, uint32_t sel,
                                                const int (&gv)[MB_MAX_PROBES][ITEMS], int p0, int ns,
                                                unsigned bias, Accum& A, unsigned long long* s_sum,
@@ -225,7 +234,7 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
 #pragma unroll
     for (int q = 0; q < MB_MAX_PROBES; ++q) {
       if (q >= (NSC >= 0 ? NSC : ns)) break;
-      const int p = p0 + q;
+      const int p = sparse_probe<ORD>(P, p0, q);
       hh += (static_cast<unsigned>(gv[q][i]) - static_cast<unsigned>(P.p_min[p])) * static_cast<unsigned>(P.p_mul[p]);
     }
     int h = static_cast<int>(hh);
@@ -239,22 +248,22 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
       const uint32_t bit = 1u << (h & 31);
       if (!(s_touch[h >> 5] & bit)) {
         if (!(atomicOr(&s_touch[h >> 5], bit) & bit) && P.res_layout != MB_RES_DENSE)
-          write_keys<NSC, ITEMS>(P, h, gv, i, p0, ns);
+          write_keys<NSC, ITEMS, ORD>(P, h, gv, i, p0, ns);
       }
     } else {
-      if (P.res_layout != MB_RES_DENSE) write_keys<NSC, ITEMS>(P, h, gv, i, p0, ns);
+      if (P.res_layout != MB_RES_DENSE) write_keys<NSC, ITEMS, ORD>(P, h, gv, i, p0, ns);
       atomicAdd(group_sum_ptr(P, h), w);
     }
   }
 }
 
-// One round of table probes: probes p0 + q for the q set in `qmask` (and q < nsp) for the
-// rows in `sel`. Every probe's loads go out before any is checked; presence is then
-// combined probe by probe in order, so selection, payloads (gv[q]) and status bits equal
-// the sequential chain.
-template <int ITEMS, class L>
-__device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint32_t& sel, int p0, int nsp,
-                                            uint32_t qmask, int (&gv)[MB_MAX_PROBES][ITEMS], Accum& A,
+// One round of table probes: probes p0 + q for q in [qlo, qhi) (and q < nsp) for the rows
+// in `sel`. Every probe's loads go out before any is checked; presence is then combined
+// probe by probe in order, so selection, payloads (gv[q]) and status bits equal the
+// sequential chain.
+template <int ITEMS, bool ORD, class L>
+__device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint32_t& sel, int p0, int nsp, int qlo,
+                                            int qhi, int (&gv)[MB_MAX_PROBES][ITEMS], Accum& A,
                                             const unsigned char* smem) {
   int v[ITEMS];
   unsigned long long sv[MB_MAX_PROBES][ITEMS];
@@ -269,8 +278,8 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
 #pragma unroll
   for (int q = 0; q < MB_MAX_PROBES; ++q) {
     if (q >= nsp) break;
-    if (!((qmask >> q) & 1u)) continue;
-    const int p = p0 + q;
+    if (q < qlo || q >= qhi) continue;
+    const int p = sparse_probe<ORD>(P, p0, q);
     ld.load(P.p_col[p], v);
     const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
     const int* ht = P.p_ht[p];
@@ -293,8 +302,8 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
 #pragma unroll
   for (int q = 0; q < MB_MAX_PROBES; ++q) {
     if (q >= nsp) break;
-    if (!((qmask >> q) & 1u)) continue;
-    const int layout = P.p_layout[p0 + q];
+    if (q < qlo || q >= qhi) continue;
+    const int layout = P.p_layout[sparse_probe<ORD>(P, p0, q)];
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
       if (!(sel & (1u << i))) continue;
@@ -313,15 +322,13 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
 }
 
 // Table probes p0 .. p0+ns-1 and the aggregate for the rows a loader exposes, in two
-// rounds: the first selective table probe alone (probe qf: the probes before it were
-// settled by their bitmaps in the dense phase and are only read for their payloads),
-// then the others together for the rows it kept (the first probe removes most rows, so
-// later tables see a fraction of the loads, at the price of one more L2 round trip). Per
-// lane: usable from divergent code.
-template <int NSC, class L>
+// rounds: the first table probe alone, then the others together for the rows it kept
+// (the first probe removes most rows, so later tables see a fraction of the loads, at
+// the price of one more L2 round trip). Per lane: usable from divergent code.
+template <int NSC, bool ORD, class L>
 __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint32_t sel, int p0, int ns,
                                             unsigned bias, Accum& A, unsigned long long* s_sum, uint32_t* s_touch,
-                                            const unsigned char* smem, int qf = 0) {
+                                            const unsigned char* smem) {
   constexpr int ITEMS = L::ITEMS;
   if (sel == 0) return;
   int gv[MB_MAX_PROBES][ITEMS];
@@ -330,13 +337,12 @@ __device__ __forceinline__ void sparse_rows(const StarPlan& P, const L& ld, uint
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) gv[q][i] = 0;
   const int nsp = NSC >= 0 ? NSC : ns;
-  const uint32_t first = 1u << qf;
-  probe_round<ITEMS>(P, ld, sel, p0, nsp, first, gv, A, smem);
+  probe_round<ITEMS, ORD>(P, ld, sel, p0, nsp, 0, 1, gv, A, smem);
   if (sel == 0) return;
-  probe_round<ITEMS>(P, ld, sel, p0, nsp, ~first, gv, A, smem);
+  probe_round<ITEMS, ORD>(P, ld, sel, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
   if (P.count_after < 0) A.cnt += __popc(sel);
   if (sel == 0) return;
-  aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
+  aggregate_rows<NSC, ITEMS, ORD>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
 }
 
 // Lane of the (k+1)-th set bit of `mask` (k < popc(mask)).
@@ -357,10 +363,10 @@ template <int NSC, int TILE, int R>
 __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const GatherLoader<TILE, R>& ld, uint32_t sel,
                                                    int p0, int ns, unsigned bias, Accum& A,
                                                    unsigned long long* s_sum, uint32_t* s_touch,
-                                                   const unsigned char* smem, int qf) {
+                                                   const unsigned char* smem) {
   const int nsp = NSC >= 0 ? NSC : ns;
   if (nsp < 2) {  // no second round to pack for
-    sparse_rows<NSC>(P, ld, sel, p0, ns, bias, A, s_sum, s_touch, smem, qf);
+    sparse_rows<NSC, true>(P, ld, sel, p0, ns, bias, A, s_sum, s_touch, smem);
     return;
   }
   const int lane = threadIdx.x & 31;
@@ -369,8 +375,7 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
   for (int q = 0; q < MB_MAX_PROBES; ++q)
 #pragma unroll
     for (int i = 0; i < R; ++i) gv0[q][i] = 0;
-  const uint32_t first = 1u << qf;
-  probe_round<R>(P, ld, sel, p0, nsp, first, gv0, A, smem);
+  probe_round<R, true>(P, ld, sel, p0, nsp, 0, 1, gv0, A, smem);
   uint32_t b[R];
   int c[R], total = 0;
 #pragma unroll
@@ -387,7 +392,7 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
       const bool mine = rem >= 0 && rem < c[i];
       const int src = mine ? nth_set_lane(b[i], rem) : lane;
       const int xr = __shfl_sync(kFull, ld.r[i], src);
-      const int xg = __shfl_sync(kFull, gv0[qf][i], src);
+      const int xg = __shfl_sync(kFull, gv0[0][i], src);
       if (mine) {
         row = xr;
         g = xg;
@@ -401,10 +406,10 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
     int gv[MB_MAX_PROBES][1];
 #pragma unroll
     for (int q = 0; q < MB_MAX_PROBES; ++q) gv[q][0] = 0;
-    gv[qf][0] = g;
-    probe_round<1>(P, l1, s1, p0, nsp, ~first, gv, A, smem);
+    gv[0][0] = g;
+    probe_round<1, true>(P, l1, s1, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
     if (P.count_after < 0) A.cnt += s1;
-    if (s1) aggregate_rows<NSC, 1>(P, l1, s1, gv, p0, ns, bias, A, s_sum, s_touch);
+    if (s1) aggregate_rows<NSC, 1, true>(P, l1, s1, gv, p0, ns, bias, A, s_sum, s_touch);
   }
 }
 
@@ -521,7 +526,7 @@ __device__ __forceinline__ void sparse_rows_mir(const StarPlan& P, const L& ld, 
     }
   }
   if (P.count_after < 0) A.cnt += __popc(sel);
-  aggregate_rows<NSC, ITEMS>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
+  aggregate_rows<NSC, ITEMS, false>(P, ld, sel, gv, p0, ns, bias, A, s_sum, s_touch);
 }
 
 // Dense phase over a warp's slice of a staged tile: lane l owns rows (j*32 + l)*4 + e,
@@ -623,7 +628,7 @@ __device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& 
   }
   if (P.count_after >= P.nf) A.cnt += sel;
   // bitmap-decided probes run here as table probes (sparse_rows consults a staged bitmap)
-  sparse_rows<-1>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
+  sparse_rows<-1, false>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
 }
 
 template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false, bool PACK = false>
@@ -778,9 +783,6 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     uint16_t* list = reinterpret_cast<uint16_t*>(smem + P.smem_list_off) + cw * WROWS;
     const int nd = P.sparse_p0;  // the sparse phase starts at probe sparse_p0 <= n_dense
     const int ns = NSC >= 0 ? NSC : P.np - P.sparse_p0;
-    // the first sparse probe that can drop rows: those before it (p < n_dense) were
-    // tested against their bitmaps in the dense phase and are read only for payloads
-    const int qf = P.n_dense - P.sparse_p0 < ns ? P.n_dense - P.sparse_p0 : 0;
     const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
     if (MIR) {
       // this CTA's share of the mirrors, visible cluster-wide after the barrier
@@ -812,9 +814,9 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
         if (MIR)
           sparse_rows_mir<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
         else if (PACK)
-          sparse_rows_packed<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, qf);
+          sparse_rows_packed<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
         else
-          sparse_rows<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, qf);
+          sparse_rows<NSC, true>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
