@@ -192,10 +192,12 @@ def tune_small(n: int = 6_000_000, copies: int = 20, reps: int = 10, verbose: bo
             "rows": n, "max_rows": 16 << 20, "best": best, "gbs": gbs, "runs": runs}
 
 
-# Shapes whose sparse phase runs the packed second round (star_kernel<..., PACK = true>):
-# measured at 120 M rows, it pays for the Query B shape (0.685 against 0.711 ms) and costs
-# the Query A (0.565 against 0.460) and engine shapes (1.03 against 0.87).
-PACKED_SHAPES = {(0, 4, 0, 1, 0)}
+# Shapes whose sparse phase runs the packed second round (star_kernel<..., PACK = true>),
+# measured at 120 M rows: the Query B shape 0.686 against 0.710 ms, the engine four-table
+# shape (customer probed first, the supplier read for its payload afterwards) 0.754
+# against 0.808 ms; the Query A shape has no packed variant (its second round is one
+# small table, and packing cost more than it saved: 0.565 against 0.460 ms).
+PACKED_SHAPES = {(0, 4, 0, 1, 0), (0, 4, 2, 1, 0)}
 
 
 def write(results: list[dict], gpu: str) -> None:
