@@ -131,6 +131,55 @@ def features(ctx: QueryContext) -> np.ndarray:
     return f
 
 
+_NPROBE = {"agg": 0, "qa": 3, "qb": 4}
+_NFILT = {"agg": 3, "qa": 1, "qb": 1}
+_OP = {"agg": L.MB_AGG_MUL, "qa": L.MB_AGG_SUM, "qb": L.MB_AGG_SUB}
+_TPL = {"agg": 0, "qa": 1, "qb": 2}
+
+
+def features_many(ctxs: list[QueryContext]) -> np.ndarray:
+    """features() of many contexts, stacked in order: the per-segment columns are computed
+    once over all of them (the per-query constants repeated), which for a window of
+    thousands of queries replaces thousands of small array programs by one."""
+    ctxs = [c for c in ctxs if len(c)]
+    if not ctxs:
+        return np.zeros((0, NUM_FEATURES), np.float32)
+    lens = np.array([len(c) for c in ctxs])
+    rep = lambda vals, dtype=np.float64: np.repeat(np.asarray(vals, dtype), lens)
+    rows = np.concatenate([np.asarray(c.rows, np.float64) for c in ctxs])
+    date_sel = np.concatenate([np.asarray(c.date_sel, np.float64) for c in ctxs])
+    resident = np.concatenate([np.asarray(c.resident_cols, np.float64) for c in ctxs])
+    sm = np.array([[c.small_sel[k] for k in ("discount", "quantity", "s", "c", "p")] for c in ctxs])
+    small = rep(np.prod(sm, axis=1))
+    sel = date_sel * small
+    needed = rep([c.needed_cols for c in ctxs])
+    missing = (needed - resident) * rows * 4
+    a = [analytic_ms(c) for c in ctxs]
+    a_cpu = np.concatenate([x[0] for x in a])
+    a_gpu = np.concatenate([x[1] for x in a])
+    tpl = rep([_TPL[c.template] for c in ctxs], np.int64)
+    f = np.empty((len(rows), NUM_FEATURES), np.float32)
+    f[:, 0:3] = np.eye(3, dtype=np.float32)[tpl]
+    f[:, 3] = np.log2(np.maximum(rows, 1))
+    f[:, 4] = date_sel
+    f[:, 5:10] = np.repeat(sm, lens, axis=0)
+    f[:, 10] = np.log10(sel + 1e-7)
+    f[:, 11] = rep([_NPROBE[c.template] for c in ctxs])
+    f[:, 12] = rep([_NFILT[c.template] for c in ctxs])
+    f[:, 13] = rep([math.log2(c.groups) for c in ctxs])
+    f[:, 14] = needed
+    f[:, 15] = resident / np.maximum(needed, 1)
+    f[:, 16] = np.log2(1 + missing / 1e6)
+    f[:, 17] = rep([math.log2(1 + c.ht_bytes / 1e6) for c in ctxs])
+    f[:, 18] = np.log2(1 + sel * rows)
+    f[:, 19] = rep([_OP[c.template] for c in ctxs])
+    f[:, 20] = rep([math.log2(max(c.cpu_threads, 1)) for c in ctxs])
+    f[:, 21] = np.log(a_cpu)
+    f[:, 22] = np.log(a_gpu)
+    f[:, 23] = rep([c.cache_free_frac for c in ctxs])
+    return f
+
+
 def place(cpu_ms: np.ndarray, gpu_ms: np.ndarray, cpu_fixed: float = 0.0, gpu_fixed: float = 0.0):
     """Split segments between the devices (mb_place_segments): returns (on_gpu, makespan)."""
     cpu_ms = np.ascontiguousarray(cpu_ms, dtype=np.float64)
@@ -221,8 +270,8 @@ class LearnedPlanner:
 
     def predict_many(self, ctxs: list[QueryContext]) -> list:
         """predict() for many queries with one model call over all their segments."""
-        feats = [features(c) for c in ctxs if len(c)]
-        y = np.exp(self.predict_log(np.concatenate(feats))) if feats else np.zeros((0, 2))
+        feats = features_many(ctxs)
+        y = np.exp(self.predict_log(feats)) if len(feats) else np.zeros((0, 2))
         out, off = [], 0
         for c in ctxs:
             fc, fg = self.fixed_ms.get(c.template, [0.0, 0.0])

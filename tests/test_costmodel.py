@@ -84,3 +84,23 @@ def test_placement_is_best_split_of_ratio_order(n, fixed):
     if n <= 10 and n > 0:  # and near the true optimum over all 2^n assignments
         opt = min(_span(cpu, gpu, np.array(m, bool), cf, gf) for m in itertools.product([0, 1], repeat=n))
         assert span.value <= opt + max(gpu.max(), cpu.max())
+
+
+def test_features_many_equals_per_query_features():
+    """The planner's stacked feature builder equals features() query by query."""
+    import numpy as np
+    from mordred_b200.planner import QueryContext, features, features_many
+    rng = np.random.default_rng(4)
+    ctxs = []
+    for k in range(40):
+        n = int(rng.integers(0, 30))
+        tpl = ("agg", "qa", "qb")[k % 3]
+        ctxs.append(QueryContext(tpl, rng.integers(1, 1 << 20, n).astype(np.float64), rng.random(n),
+                                 {x: float(rng.random()) for x in ("discount", "quantity", "s", "c", "p")},
+                                 {"agg": 4, "qa": 4, "qb": 6}[tpl], rng.integers(0, 5, n).astype(np.int32),
+                                 int(rng.integers(0, 1 << 24)), 1000, {"agg": 1, "qa": 7000, "qb": 175}[tpl],
+                                 16, float(rng.random())))
+    want = np.concatenate([features(c) for c in ctxs if len(c)])
+    got = features_many(ctxs)
+    assert got.shape == want.shape
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
