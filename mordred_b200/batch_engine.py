@@ -259,17 +259,20 @@ class BatchExecutor(CpuShare):
         cands = [self.candidates(q) for q in queries]
         (preds, saving) = self._predict(planner, queries, cands)
         copied = self._admit(queries, cands, saving, ks) if saving is not None else 0
-        # per segment: the queries that need it, their CPU ms (with build shares), the batch's GPU ms
-        need: dict[int, list] = {}
-        for qi, (cand, (pc, pg, fc, fg)) in enumerate(zip(cands, preds)):
-            for j, s in enumerate(cand):
-                need.setdefault(int(s), []).append((qi, pc[j] + fc / len(cand), pg[j]))
-        segs = np.array(sorted(need), np.int64)
-        if len(segs):
-            cpu_cost = np.array([sum(x[1] for x in need[s]) for s in segs])
-            gpu_cost = np.array([max(x[2] for x in need[s]) for s in segs])
+        # per segment: the CPU ms of the queries that need it (each with its share of the
+        # query's host builds) summed, and the most expensive member's GPU ms
+        nz = [(np.asarray(c, np.int64), pc, pg, fc) for c, (pc, pg, fc, fg) in zip(cands, preds) if len(c)]
+        if nz:
+            seg_all = np.concatenate([c for c, _, _, _ in nz])
+            cpu_all = np.concatenate([np.asarray(pc, np.float64) + fc / len(c) for c, pc, _, fc in nz])
+            gpu_all = np.concatenate([np.asarray(pg, np.float64) for _, _, pg, _ in nz])
+            segs, inv = np.unique(seg_all, return_inverse=True)
+            cpu_cost = np.bincount(inv, weights=cpu_all, minlength=len(segs))
+            gpu_cost = np.full(len(segs), -np.inf)
+            np.maximum.at(gpu_cost, inv, gpu_all)
             on_gpu, span = place(cpu_cost, gpu_cost)
         else:
+            segs = np.zeros(0, np.int64)
             on_gpu, span = np.zeros(0, bool), 0.0
         gsegs, csegs = segs[on_gpu], segs[~on_gpu]
         plan_ms = (time.perf_counter() - t0) * 1e3
