@@ -391,22 +391,25 @@ def planner_section(args, table=None):
     # the whole workload as one window: every staged segment is copied once for all the
     # queries (up to 256 a launch) instead of once per window of 256
     whole_res = {}
-    one_window = PE.evaluate_batched(bx, [learned], queries, start, window=len(queries), log=lambda *a: None,
-                                     keep_results=whole_res)
+    one_window = PE.evaluate_batched(bx, [AnalyticPlanner(), learned], queries, start, window=len(queries),
+                                     log=lambda *a: None, keep_results=whole_res)
     bx.close()
     bx.cache.close()
     del bx
     torch.cuda.empty_cache()
     ref = plain_res["analytic"]
     identical = all(all(np.array_equal(a, b) for a, b in zip(ref, r)) for r in
-                    [plain_res["learned"], batch_res["analytic"], batch_res["learned"], whole_res["learned"]])
+                    [plain_res["learned"], batch_res["analytic"], batch_res["learned"], whole_res["analytic"],
+                     whole_res["learned"]])
     base = plain["analytic"]["total_ms"]
     return {"fact_rows": args.planner_rows, "segments": table.nseg, "cache_slots": slots,
             "queries": len(queries), "setup_s": setup_s,
             "plain_analytic_ms": base, "plain_learned_ms": plain["learned"]["total_ms"],
             "batched_analytic_ms": batched["analytic"]["total_ms"],
             "batched_learned_ms": batched["learned"]["total_ms"],
+            "batched_analytic_one_window_ms": one_window["analytic"]["total_ms"],
             "batched_learned_one_window_ms": one_window["learned"]["total_ms"],
+            "speedup_batched_learned_one_window_vs_plain_analytic": base / one_window["learned"]["total_ms"],
             "speedup_batched_learned_vs_plain_analytic": base / batched["learned"]["total_ms"],
             "speedup_learned_vs_analytic_plain": base / plain["learned"]["total_ms"],
             "speedup_learned_vs_analytic_batched": batched["analytic"]["total_ms"] / batched["learned"]["total_ms"],
@@ -523,7 +526,8 @@ def summary_of(per_query, batched, planner, serving) -> dict:
     if planner and "plain_analytic_ms" in planner:
         out["config3_queries"] = planner["queries"]
         for k in ("plain_analytic_ms", "plain_learned_ms", "batched_analytic_ms", "batched_learned_ms",
-                  "batched_learned_one_window_ms", "speedup_batched_learned_vs_plain_analytic",
+                  "batched_analytic_one_window_ms", "batched_learned_one_window_ms",
+                  "speedup_batched_learned_vs_plain_analytic", "speedup_batched_learned_one_window_vs_plain_analytic",
                   "results_identical_all_forms"):
             out["config3_" + k] = planner[k]
         live = planner["prediction_mae_live"]
