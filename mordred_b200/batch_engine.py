@@ -113,9 +113,8 @@ class BatchExecutor(CpuShare):
         segments, and — for admission — the predicted GPU ms each segment saves when its
         columns are resident rather than missing (batched model calls)."""
         ctxs = [self.context(q, c) for q, c in zip(queries, cands)]
-        base = planner.predict_many(ctxs)
         if not self.admission:
-            return base, None
+            return planner.predict_many(ctxs), None
         lo, hi = [], []
         for ctx in ctxs:
             a = ctx.subset(slice(None))
@@ -124,8 +123,10 @@ class BatchExecutor(CpuShare):
             b.resident_cols = np.full_like(ctx.resident_cols, ctx.needed_cols)
             lo.append(a)
             hi.append(b)
-        miss = planner.predict_many(lo)
-        res = planner.predict_many(hi)
+        # one model call for the window's three views (as cached, all missing, all resident)
+        out = planner.predict_many(ctxs + lo + hi)
+        n = len(ctxs)
+        base, miss, res = out[:n], out[n: 2 * n], out[2 * n:]
         saving = [np.maximum(m[1] - r[1], 0.0) for m, r in zip(miss, res)]
         return base, saving
 
