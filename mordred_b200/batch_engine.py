@@ -112,7 +112,8 @@ class BatchExecutor(CpuShare):
         """Per query, the planner's (cpu_ms, gpu_ms, cpu_fixed, gpu_fixed) over its candidate
         segments, and — for admission — the predicted GPU ms each segment saves when its
         columns are resident rather than missing (batched model calls)."""
-        ctxs = [self.context(q, c) for q, c in zip(queries, cands)]
+        snap = self.residency()
+        ctxs = [self.context(q, c, snap) for q, c in zip(queries, cands)]
         if not self.admission:
             return planner.predict_many(ctxs), None
         lo, hi = [], []

@@ -238,10 +238,18 @@ class CpuShare:
                       segment_size=SEG)
         cpu.star_query(a, nthreads=self.cpu_nthreads)
 
-    def context(self, q: B.Query, segs: np.ndarray) -> QueryContext:
+    def residency(self) -> tuple[dict, float]:
+        """The cache's residency as context() reads it — per column, the slot of every
+        segment (< 0: not resident) — and its free share: one snapshot for the many
+        contexts a window plans at once."""
+        idx = {c: self.cache.col_idx(COL_ID[c]) for c in FACT}
+        return idx, 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
+
+    def context(self, q: B.Query, segs: np.ndarray, snapshot: tuple | None = None) -> QueryContext:
         """The planners' view of q over `segs`: rows, in-range share of each segment's
         rows (the table is date-sorted, so a segment's dates are contiguous), residency of
-        the needed columns, hash-table sizes. Needs `cache` and `cpu_threads` too."""
+        the needed columns, hash-table sizes. Needs `cache` and `cpu_threads` too;
+        `snapshot` (from residency()) saves reading the cache for every query."""
         t = self.t
         segs = np.asarray(segs, np.int64)
         lo, hi = t.seg_day_lo[segs], t.seg_day_hi[segs]
@@ -251,12 +259,13 @@ class CpuShare:
         need = NEEDED[q.template]
         res = np.zeros(len(segs), np.int32)
         for c in need:
-            res += self.cache.col_idx(COL_ID[c])[segs] >= 0
+            idx = snapshot[0][c] if snapshot is not None else self.cache.col_idx(COL_ID[c])
+            res += idx[segs] >= 0
         s = t.sizes
         ht_bytes = {"agg": 0, "qa": 4 * (s.s_len + 2 * s.p_len + 2 * ssb.DATE_SLOTS),
                     "qb": 4 * (s.s_len + 2 * s.c_len + s.p_len + 2 * ssb.DATE_SLOTS)}[q.template]
         dim_rows = {"agg": 0, "qa": s.s_len + s.p_len + s.d_len, "qb": s.s_len + s.c_len + s.p_len + s.d_len}
-        free = 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
+        free = snapshot[1] if snapshot is not None else 1.0 - self.cache.stats()["resident"] / self.cache.num_slots
         return QueryContext(q.template, t.seg_rows[segs].astype(np.float64), date_sel.astype(np.float64),
                             _small_sel(q), len(need), res, ht_bytes, dim_rows[q.template], q.groups,
                             self.cpu_threads, free)
