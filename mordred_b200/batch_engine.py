@@ -71,6 +71,8 @@ class BatchExecutor(CpuShare):
     """Windows of queries over a :class:`SegmentedTable` with a GPU segment cache of
     `cache_slots` slots (the budget includes the staging slots)."""
 
+    MAX_CHUNKS = 16  # 256-query launches a window may hold (4,096 queries)
+
     def __init__(self, table: SegmentedTable, cache_slots: int = 2048, stage_segments: int = 12, device: int = 0,
                  benefit_decay: float = 0.5):
         ncol = len(FACT)
@@ -93,8 +95,11 @@ class BatchExecutor(CpuShare):
         # behind the previous window's scans while the next window is being enqueued
         self.col_h = torch.empty(2, self.max_waves, ncol, table.nseg, dtype=torch.int32, pin_memory=True)
         self.col_d = torch.empty(self.max_waves, ncol, table.nseg, dtype=torch.int32, device="cuda")
-        self.seg_h = torch.empty(2, self.max_waves, table.nseg, dtype=torch.int16, pin_memory=True)
-        self.seg_d = torch.empty(self.max_waves, table.nseg, dtype=torch.int16, device="cuda")
+        # per wave and query chunk (up to 256 queries a launch): the wave's segments that the
+        # chunk's queries can match
+        self.seg_h = torch.empty(2, self.max_waves, self.MAX_CHUNKS, table.nseg, dtype=torch.int16,
+                                 pin_memory=True)
+        self.seg_d = torch.empty(self.max_waves, self.MAX_CHUNKS, table.nseg, dtype=torch.int16, device="cuda")
         self._parity = 0
         self._stage_done = [None, None]  # events: the last scans that read staging buffer 0 / 1
         self._stage_buf = 0
@@ -148,14 +153,17 @@ class BatchExecutor(CpuShare):
         return self.cache.stats()["admissions"] - before
 
     # ---- GPU share -------------------------------------------------------------------------
-    def _launch(self, w: int, segs: np.ndarray, qarrs: list, cols_needed: list[int], stream) -> int:
-        """One batched launch per chunk of up to 256 queries over the wave's segments
-        (col_d[w] / seg_d[w] already hold its slot arrays); returns launches issued."""
-        n_rows = self._rows(segs)
+    def _launch(self, w: int, subsets: list, qarrs: list, cols_needed: list[int], stream) -> int:
+        """One batched launch per chunk of up to 256 queries over the wave's segments that
+        chunk can match (col_d[w] / seg_d[w, k] already hold the slot arrays and segment
+        lists); returns launches issued."""
         launches = 0
-        for arr, nq, cols in qarrs:
+        for k, (arr, nq, cols, _) in enumerate(qarrs):
+            sub = subsets[k]
+            if len(sub) == 0:
+                continue
             a = L.MbBatchArgs()
-            a.num_rows = n_rows
+            a.num_rows = self._rows(sub)
             for c in cols:
                 a.fact[c] = self.col_d[w, c].data_ptr()
             a.dim = self.c_dims
@@ -163,7 +171,7 @@ class BatchExecutor(CpuShare):
             a.queries = C.cast(arr, C.POINTER(L.MbBatchQuery))
             a.smem_group_bytes = -1
             a.gpu_cache = self.cache.pool
-            a.segment_group = self.seg_d[w].data_ptr()
+            a.segment_group = self.seg_d[w, k].data_ptr()
             a.segment_size = SEG
             need = int(L.lib().mb_batch_workspace_bytes(C.byref(a)))
             if need > self.ws.numel():
@@ -212,11 +220,14 @@ class BatchExecutor(CpuShare):
                 copied = torch.cuda.Event()
                 copied.record(cs)
                 ks.wait_event(copied)
-            seg_h[w, : len(segs)] = torch.from_numpy(segs.astype(np.int16))
+            subsets = [segs[mask[segs]] for _, _, _, mask in qarrs]  # keeps the partial segment last
             with torch.cuda.stream(ks):
                 self.col_d[w].copy_(col_h[w], non_blocking=True)
-                self.seg_d[w, : len(segs)].copy_(seg_h[w, : len(segs)], non_blocking=True)
-            launches += self._launch(w, segs, qarrs, cols_needed, ks)
+                for k, sub in enumerate(subsets):
+                    if len(sub):
+                        seg_h[w, k, : len(sub)] = torch.from_numpy(sub.astype(np.int16))
+                        self.seg_d[w, k, : len(sub)].copy_(seg_h[w, k, : len(sub)], non_blocking=True)
+            launches += self._launch(w, subsets, qarrs, cols_needed, ks)
             if needs_stage:
                 ev = torch.cuda.Event()
                 ev.record(ks)
@@ -283,13 +294,26 @@ class BatchExecutor(CpuShare):
         # for) and launch descriptors (chunks of up to 256 queries)
         flat, views = B.result_buffers(queries)
         ks.wait_stream(torch.cuda.current_stream())
+        # launch chunks of up to 256 queries, grouped by the part of the date-sorted table
+        # they need (queries over more than a quarter of it together, the others by their
+        # first segment), so that each chunk's launch scans only the segments its queries
+        # can match instead of every segment the window scans
+        nseg = self.t.nseg
+        order = sorted(range(len(queries)),
+                       key=lambda i: (len(cands[i]) > nseg // 4, int(cands[i][0]) if len(cands[i]) else -1,
+                                      len(cands[i])))
         qarrs = []
-        for base in range(0, len(queries), L.MB_BATCH_MAX_QUERIES):
-            chunk = list(range(base, min(len(queries), base + L.MB_BATCH_MAX_QUERIES)))
+        for base in range(0, len(order), L.MB_BATCH_MAX_QUERIES):
+            chunk = order[base: base + L.MB_BATCH_MAX_QUERIES]
             arr = (L.MbBatchQuery * len(chunk))(*[queries[i].to_c(views[i]) for i in chunk])
             cols = sorted({COL_ID[c] for i in chunk for c in NEEDED[queries[i].template]})
-            qarrs.append((arr, len(chunk), cols))
-        cols_needed = sorted({c for _, _, cols in qarrs for c in cols})
+            mask = np.zeros(nseg, bool)
+            for i in chunk:
+                mask[cands[i]] = True
+            qarrs.append((arr, len(chunk), cols, mask))
+        if len(qarrs) > self.MAX_CHUNKS:
+            raise ValueError(f"a window holds at most {self.MAX_CHUNKS * L.MB_BATCH_MAX_QUERIES} queries")
+        cols_needed = sorted({c for _, _, cols, _ in qarrs for c in cols})
 
         # CPU share on the CPU worker: per query, its host tables and its CPU segments
         host_res = [np.zeros(2 if q.template == "agg" else 4 * q.groups, np.int32) for q in queries]

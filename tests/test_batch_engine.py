@@ -88,3 +88,24 @@ def test_admission_keeps_demanded_segments_resident(table):
     ex.close()
     assert runs[0].copied_column_segments > 0
     assert all(w.staged_segments == 0 for w in runs[1:])
+
+
+def test_one_window_of_several_launch_chunks(table):
+    """A window of 300 queries (two 256-query launch chunks, each scanning only the
+    segments its queries can match) equals the oracle query by query, all on the GPU and
+    under the analytic planner's split."""
+    from mordred_b200 import _lib as L
+    from mordred_b200.batch_engine import BatchExecutor
+    from mordred_b200.planner import AnalyticPlanner
+    from query_oracle import expected
+    qs = B.generate_queries(300, seed=707, sel_lo=1e-4, sel_hi=0.3)
+    h = _host(table)
+    exp = [expected(h, table.sizes, q).view(np.int32) for q in qs]
+    ex = BatchExecutor(table, cache_slots=40 + 2 * 2 * 9, stage_segments=2)
+    for planner in (_Fixed("gpu", True), AnalyticPlanner()):
+        runs = ex.run(qs, planner, window=len(qs))
+        assert len(runs) == 1 and runs[0].launches >= 2
+        for i, (g, e) in enumerate(zip(runs[0].results, exp)):
+            assert np.array_equal(g, e), (planner.name, i, qs[i].template)
+    ex.close()
+    assert L.device_status(0) == 0
