@@ -317,16 +317,18 @@ class BatchExecutor(CpuShare):
 
         # CPU share on the CPU worker: per query, its host tables and its CPU segments
         host_res = [np.zeros(2 if q.template == "agg" else 4 * q.groups, np.int32) for q in queries]
-        cseg_set = set(int(s) for s in csegs)
+        on_cpu = np.zeros(self.t.nseg, bool)
+        on_cpu[csegs] = True
         cpu_ms = [0.0]
 
         def cpu_share():
             c0 = time.perf_counter()
             for qi, (q, cand) in enumerate(zip(queries, cands)):
-                mine = [int(s) for s in cand if int(s) in cseg_set]
-                if mine:
+                mine = np.asarray(cand, np.int64)
+                mine = mine[on_cpu[mine]] if len(mine) else mine
+                if len(mine):
                     self.build_cpu(q)
-                    self._cpu_segments(q, mine, host_res[qi])
+                    self._cpu_segments(q, [int(x) for x in mine], host_res[qi])
             cpu_ms[0] = (time.perf_counter() - c0) * 1e3
 
         cpu_done, cpu_err = threading.Event(), []
