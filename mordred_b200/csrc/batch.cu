@@ -71,11 +71,6 @@ struct __align__(16) AQ {
 __device__ __forceinline__ int aq_family(const AQ& A) { return (A.flags >> 8) & 0x1ff; }
 __device__ __forceinline__ int aq_member(const AQ& A) { return (A.flags >> 17) & 0x1ff; }
 static_assert(sizeof(AQ) == 32, "aggregation descriptor size");
-// Descriptors sit in shared memory 48 bytes apart: a 16-byte load of query q then starts
-// in bank group 3q mod 8, so the eight lanes of one access phase reading neighbouring
-// queries (one row's matches) hit eight different groups, where a 32-byte stride (2q mod
-// 8) reaches only four.
-constexpr int kAqStrideWords = 12;
 
 // Per-query descriptor in the launch parameters (96 bytes).
 struct BQ {
@@ -173,7 +168,7 @@ __device__ __forceinline__ void bmbar_arrive(uint64_t* bar) {
 }
 
 __device__ __forceinline__ AQ load_aq(const AQ* s_aq, int qi) {
-  const uint4* p = reinterpret_cast<const uint4*>(reinterpret_cast<const unsigned*>(s_aq) + qi * kAqStrideWords);
+  const uint4* p = reinterpret_cast<const uint4*>(s_aq + qi);
   const uint4 x = p[0], y = p[1];
   AQ a;
   a.a0 = static_cast<uint16_t>(x.x);
@@ -311,8 +306,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
     for (int w = tid; w < P.acc_words; w += NWARPS * 32) s_acc[w] = 0;
     for (int q = tid; q < P.nq; q += NWARPS * 32) s_res[q] = P.q[q].res;
     unsigned* dst = reinterpret_cast<unsigned*>(s_aq);
-    for (int w = tid; w < P.nq * 8; w += NWARPS * 32)
-      dst[(w >> 3) * kAqStrideWords + (w & 7)] = reinterpret_cast<const unsigned*>(&P.q[w >> 3].a)[w & 7];
+    for (int w = tid; w < P.nq * 8; w += NWARPS * 32) dst[w] = reinterpret_cast<const unsigned*>(&P.q[w >> 3].a)[w & 7];
     for (int w = tid; w < 16 * kMaskWordsMax; w += NWARPS * 32) s_pres[w] = (&P.pres_mask[0][0])[w];
     for (int w = tid; w < kMaxPredFields * kMaskWordsMax; w += NWARPS * 32) s_out[w] = (&P.outside[0][0])[w];
     unsigned* g = reinterpret_cast<unsigned*>(smem + P.smem_groups_off);
@@ -574,7 +568,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
   // ---- fold this CTA's scalars and shared-memory group arrays into the results -------
   // (a zero partial is skipped: adding it changes nothing)
   for (int q = 0; q < P.nq; ++q) {
-    const AQ A = load_aq(s_aq, q);
+    const AQ A = s_aq[q];
     if (A.soff < 0) continue;
     const unsigned long long* s_sum = reinterpret_cast<const unsigned long long*>(smem + A.soff);
     const bool c4 = (A.flags >> 2) & 1;
@@ -959,7 +953,7 @@ extern "C" int mb_batch_run(const mb_batch_args* a, mb_stream_t stream) {
   off += 8 * P.acc_words;
   off = (off + 15) / 16 * 16;
   P.smem_aq_off = off;
-  off += 4 * kAqStrideWords * P.nq;
+  off += static_cast<int>(sizeof(AQ)) * P.nq;
   P.smem_res_off = off;
   off += 8 * P.nq;
   off = (off + 15) / 16 * 16;
