@@ -145,8 +145,10 @@ typedef struct mb_star_args {
   int mirrors;
   /* Second sparse round packed across the warp (the rows the first selective table probe
    * kept are moved one a lane before the later probes and the aggregate run): 0 = the
-   * tuned default for the shape, 1 = never, 2 = where the shape has a packed variant.
-   * Results are the same either way. */
+   * tuned default for the shape, 1 = never, 2 = where the shape has a packed variant,
+   * 3 = packed, with each tile's stage handed back to the bulk-copy producer before its
+   * last batch of survivors is probed (their columns held in registers). Results are the
+   * same either way. */
   int pack;
 } mb_star_args;
 

@@ -26,6 +26,7 @@ HEADER = os.path.join(HERE, "csrc", "tuned_configs.h")
 JSON = os.path.join(HERE, "tuned_configs.json")
 
 THREADS = (128, 256, 512)
+WIDE_THREADS = (640, 768)  # 20 and 24 consumer warps over 16 tile slices (packed shapes only)
 ITEMS = (4, 8, 16)
 STAGES = (2, 3, 4, 6)
 
@@ -125,15 +126,20 @@ def tune(n: int = 120_000_000, reps: int = 5, verbose: bool = True) -> list[dict
     results = []
     for name, bpr, key, make in shapes:
         runs = []
-        for th, it, stg, gm in itertools.product(THREADS, ITEMS, STAGES, (1, 2)):
+        packed = tuple(key) in PACKED_SHAPES
+        threads = THREADS + (WIDE_THREADS if packed else ())
+        # mb_star_args.pack: 1 plain, 2 packed, 3 packed with early stage return
+        packs = (1, 2, 3) if packed else (1,)
+        for th, it, stg, gm, pk in itertools.product(threads, ITEMS, STAGES, (1, 2), packs):
             if key[3] == 0 and gm == 2:
                 continue  # scalar results have no group array
             try:
-                a = make(threads=th, items_per_thread=it, stages=stg, group_mode=gm if key[3] else 0)
+                a = make(threads=th, items_per_thread=it, stages=stg, group_mode=gm if key[3] else 0, pack=pk)
                 ms = _time(lambda: ssb.star_query(a), reps)
             except L.MbError:
                 continue
-            runs.append({"threads": th, "items": it, "stages": stg, "group_mode": gm if key[3] else 0, "ms": ms})
+            runs.append({"threads": th, "items": it, "stages": stg, "group_mode": gm if key[3] else 0,
+                         "pack": pk - 1, "ms": ms})
         runs.sort(key=lambda r: r["ms"])
         best = runs[0]
         gbs = n * bpr / best["ms"] / 1e6
@@ -196,7 +202,11 @@ def tune_small(n: int = 6_000_000, copies: int = 20, reps: int = 10, verbose: bo
 # measured at 120 M rows: the Query B shape 0.686 against 0.710 ms, the engine four-table
 # shape (customer probed first, the supplier read for its payload afterwards) 0.754
 # against 0.808 ms; the Query A shape has no packed variant (its second round is one
-# small table, and packing cost more than it saved: 0.565 against 0.460 ms).
+# small table, and packing cost more than it saved: 0.565 against 0.460 ms). These shapes
+# also have the variants that return each stage before the last batch's probes
+# (REL = true) and run 20 or 24 consumer warps over 16 tile slices: Query B 0.627 against
+# 0.724 ms, the engine shape 0.666 against 0.795 ms for the 16-warp packed kernel (same
+# box). The tuned entry's pack field: 1 packed, 2 packed with early stage return.
 PACKED_SHAPES = {(0, 4, 0, 1, 0), (0, 4, 2, 1, 0)}
 
 
@@ -205,7 +215,7 @@ def write(results: list[dict], gpu: str) -> None:
     for r in sorted(results, key=lambda r: -r.get("max_rows", 0)):  # row-limited entries first
         b, k = r["best"], r["key"]
         limit = f", {r['max_rows'] >> 20}ll << 20" if r.get("max_rows") else ""
-        pack = ", 0, 1" if tuple(k) in PACKED_SHAPES else ""
+        pack = f", 0, {b['pack']}" if b.get("pack") else ""
         lines.append(f"    {{{k[0]}, {k[1]}, {k[2]}, {k[3]}, {k[4]}, {{{b['threads']}, {b['items']}, {b['stages']}, "
                      f"{b['group_mode']}{pack}}}{limit}}},  // {r['shape']}: {b['ms']:.4f} ms, {r['gbs'] / 1000:.2f} TB/s")
     text = open(HEADER).read()

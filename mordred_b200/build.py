@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmordred_b200.so")
 
-SOURCES = ["capi.cu", "star.cu", "star_special.cu", "build.cu", "listq.cu", "noalloc.cu", "batch.cu", "compact.cu", "mlp.cu", "cpu_engine.cpp",
+SOURCES = ["capi.cu", "star.cu", "star_special.cu", "star_wide.cu", "build.cu", "listq.cu", "noalloc.cu", "batch.cu", "compact.cu", "mlp.cu", "cpu_engine.cpp",
            "segcache.cpp", "costmodel.cpp"]
 # host code: portable x86-64 with AVX2 (the library is built on one machine and run on another)
 HOST_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-pthread"]

@@ -23,14 +23,18 @@ const Variant* star_variants_generic(int* count) {
 
 // The specialised variant for this shape if one was compiled, else the generic one. The
 // mirror-reading variants exist for specialised shapes only.
-static const Variant* find_variant(int warps, int items, int nf, int nd, int ns, bool mir, bool pack = false) {
+static const Variant* find_variant(int warps, int items, int nf, int nd, int ns, bool mir, bool pack = false,
+                                   bool rel = false) {
   int n = 0;
-  const Variant* sp = star_variants_special(&n);
-  for (int i = 0; i < n; ++i)
-    if (sp[i].warps == warps && sp[i].items == items && sp[i].nf == nf && sp[i].nd == nd && sp[i].ns == ns &&
-        sp[i].mir == mir && sp[i].pack == pack)
-      return &sp[i];
+  for (int t = 0; t < 2; ++t) {
+    const Variant* sp = t == 0 ? star_variants_special(&n) : star_variants_wide(&n);
+    for (int i = 0; i < n; ++i)
+      if (sp[i].warps == warps && sp[i].items == items && sp[i].nf == nf && sp[i].nd == nd && sp[i].ns == ns &&
+          sp[i].mir == mir && sp[i].pack == pack && sp[i].rel == rel)
+        return &sp[i];
+  }
   if (mir) return nullptr;
+  if (rel) return find_variant(warps, items, nf, nd, ns, false, true, false);  // no early-release variant
   if (pack) return find_variant(warps, items, nf, nd, ns, false, false);  // no packing variant: plain one
   const Variant* g = star_variants_generic(&n);
   for (int i = 0; i < n; ++i)
@@ -39,9 +43,9 @@ static const Variant* find_variant(int warps, int items, int nf, int nd, int ns,
 }
 
 int star_init_device(const DeviceState& ds) {
-  for (int t = 0; t < 2; ++t) {
+  for (int t = 0; t < 3; ++t) {
     int n = 0;
-    const Variant* v = t == 0 ? star_variants_generic(&n) : star_variants_special(&n);
+    const Variant* v = t == 0 ? star_variants_generic(&n) : t == 1 ? star_variants_special(&n) : star_variants_wide(&n);
     for (int i = 0; i < n; ++i) {
       cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(v[i].fn),
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, ds.max_smem_optin - 2048);
@@ -63,8 +67,8 @@ static int round_up(int x, int a) { return (x + a - 1) / a * a; }
 // Lay out shared memory for `stages` stages; returns total bytes. A mirror share (P.cluster >
 // 1) sits between the survivor lists and the stage ring.
 static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_bitmaps) {
-  const int tile = ncw * 32 * items;
-  int off = 2 * kMaxStages * 8;  // full and empty mbarriers
+  const int tile = tile_slices(ncw) * 32 * items;
+  int off = 3 * kMaxStages * 8;  // full (two per stage) and empty mbarriers
   P.smem_groups_off = off;
   if (P.gmode == kGroupSmem) off += round_up(8 * P.total_val + 4 * ((P.total_val + 31) / 32), 128);
   int bm_total = 0;
@@ -262,10 +266,10 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   const TunedConfig tc = tuned_config(P.nf, a->num_probes, a->probe[0].layout, P.res_layout, P.total_val, P.n);
   const int threads = a->threads ? a->threads : tc.threads;
   const int items = a->items_per_thread ? a->items_per_thread : tc.items;
-  if (threads % 32 != 0 || threads < 128 || threads > 512) return MB_ERR_ARG;
+  if (threads % 32 != 0 || threads < 128 || threads > 768) return MB_ERR_ARG;
   if (items != 4 && items != 8 && items != 16) return MB_ERR_ARG;
   const int ncw = threads / 32;
-  const int tile = threads * items;
+  const int tile = tile_slices(ncw) * 32 * items;
   if (P.gpu_cache != nullptr && (1 << P.seg_shift) < tile) return MB_ERR_ARG;
 
   bool direct_aligned = true;
@@ -283,8 +287,9 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   if (group_mode == 1 && P.gmode != kGroupSmem) return MB_ERR_SIZE;
 
   if (a->mirrors < 0 || a->mirrors > 2) return MB_ERR_ARG;
-  if (a->pack < 0 || a->pack > 2) return MB_ERR_ARG;
-  const bool want_pack = a->pack == 2 || (a->pack == 0 && tc.pack != 0);
+  if (a->pack < 0 || a->pack > 3) return MB_ERR_ARG;
+  const bool want_pack = a->pack >= 2 || (a->pack == 0 && tc.pack != 0);
+  const bool want_rel = a->pack == 3 || (a->pack == 0 && tc.pack == 2);
   const int budget = ds->max_smem_optin - 2048 - 2 * 8 * (ncw + 1);
   const int want_stages = a->stages ? a->stages : tc.stages;
   if (want_stages < 2 || want_stages > kMaxStages) return MB_ERR_ARG;
@@ -318,7 +323,8 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   }
   if (smem > budget) smem = layout_smem(P, ncw, items, 2, false);
   if (smem > budget) return MB_ERR_SIZE;
-  if (var == nullptr) var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, want_pack);
+  if (var == nullptr)
+    var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, want_pack, want_rel);
   if (var == nullptr) return MB_ERR_ARG;
 
   // sparse visiting order of the tiled path: chain order, except that the first probe

@@ -25,6 +25,13 @@ namespace mb {
 
 constexpr int kMaxCols = MB_MAX_FILTERS + MB_MAX_PROBES + 2;
 constexpr int kMaxStages = 8;
+// A staged tile is cut into slices of 32 x items rows, one per consumer warp; launches with
+// more than 16 consumer warps keep 16 slices a tile and hand the slices out round robin, so
+// several warps probe earlier slices while others run the dense phase of later ones.
+constexpr int kMaxTileSlices = 16;
+__host__ __device__ constexpr int tile_slices(int consumer_warps) {
+  return consumer_warps > kMaxTileSlices ? kMaxTileSlices : consumer_warps;
+}
 constexpr int kSmemGroupMax = 8192;            // groups kept in shared memory per CTA
 constexpr int kBitmapSmemMaxBytes = 32768;     // largest presence bitmap staged (262,144 slots)
 constexpr int kBitmapSmemTotalBytes = 40960;

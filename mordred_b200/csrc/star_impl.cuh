@@ -24,6 +24,7 @@ struct Variant {
   KernelFn fn;
   bool mir = false;   // reads cluster-resident mirrors (launched with a cluster)
   bool pack = false;  // packs the first sparse probe's survivors across the warp
+  bool rel = false;   // packed, and returns each stage before its last batch's probes
 };
 
 __device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
@@ -144,15 +145,34 @@ __device__ __forceinline__ const int* row_ptr(const StarPlan& P, int c, long lon
   return P.gpu_cache + (slot << P.seg_shift) + (r & ((1ll << P.seg_shift) - 1));
 }
 
+// Loaders hand the sparse phase a column's values for the rows it holds: load(slot, c, v)
+// reads staged column c. `slot` names the column's role — sparse position q for a probe
+// key, kAggSlot + a for aggregate column a — and is a compile-time constant after
+// unrolling; only RegLoader uses it.
+constexpr int kAggSlot = MB_MAX_PROBES;
+constexpr int kLoadSlots = MB_MAX_PROBES + 2;
+
 // Survivors gathered from a staged tile through a warp's row list.
 template <int TILE, int R>
 struct GatherLoader {
   static constexpr int ITEMS = R;
   const int* wstage;
   int r[R];
-  __device__ __forceinline__ void load(int c, int (&v)[R]) const {
+  __device__ __forceinline__ void load(int, int c, int (&v)[R]) const {
 #pragma unroll
     for (int i = 0; i < R; ++i) v[i] = wstage[c * TILE + r[i]];
+  }
+};
+
+// Survivors whose columns were copied into registers (the stage they came from already
+// returned to the producer).
+template <int R>
+struct RegLoader {
+  static constexpr int ITEMS = R;
+  int val[kLoadSlots][R];
+  __device__ __forceinline__ void load(int slot, int, int (&v)[R]) const {
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = val[slot][i];
   }
 };
 
@@ -161,7 +181,7 @@ struct RowLoader {
   static constexpr int ITEMS = 1;
   const StarPlan* P;
   long long r;
-  __device__ __forceinline__ void load(int c, int (&v)[1]) const { v[0] = __ldg(row_ptr(*P, c, r)); }
+  __device__ __forceinline__ void load(int, int c, int (&v)[1]) const { v[0] = __ldg(row_ptr(*P, c, r)); }
 };
 
 // Probe index of sparse position q. The tiled path visits its sparse probes in the
@@ -211,8 +231,8 @@ __device__ __forceinline__ void aggregate_rows(const StarPlan& P, const L& ld, u
                                                unsigned bias, Accum& A, unsigned long long* s_sum,
                                                uint32_t* s_touch) {
   int a0[ITEMS], a1[ITEMS];
-  ld.load(P.a_col[0], a0);
-  if (P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL) ld.load(P.a_col[1], a1);
+  ld.load(kAggSlot, P.a_col[0], a0);
+  if (P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL) ld.load(kAggSlot + 1, P.a_col[1], a1);
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     if (!(sel & (1u << i))) continue;
@@ -280,7 +300,7 @@ __device__ __forceinline__ void probe_round(const StarPlan& P, const L& ld, uint
     if (q >= nsp) break;
     if (q < qlo || q >= qhi) continue;
     const int p = sparse_probe<ORD>(P, p0, q);
-    ld.load(P.p_col[p], v);
+    ld.load(q, P.p_col[p], v);
     const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p];
     const int* ht = P.p_ht[p];
     const uint32_t* bm = P.p_bm_off[p] >= 0 ? reinterpret_cast<const uint32_t*>(smem + P.p_bm_off[p]) : nullptr;
@@ -413,6 +433,79 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
   }
 }
 
+// sparse_rows_packed for a warp's last batch of a tile, returning the stage early: the
+// survivors' columns that the sparse phase reads (every sparse probe key and the
+// aggregate operands) are copied into registers, `release()` hands the stage back to
+// the producer, and the two probe rounds — with their L2 round trips — run from
+// registers while the next tile lands. After the first probe the kept rows are packed
+// across the warp with all their column values (shuffles), as in sparse_rows_packed.
+// Warp-converged: every lane calls it.
+template <int NSC, int TILE, int R, class Release>
+__device__ __forceinline__ void sparse_rows_packed_regs(const StarPlan& P, const GatherLoader<TILE, R>& gl,
+                                                        uint32_t sel, int p0, int ns, unsigned bias, Accum& A,
+                                                        unsigned long long* s_sum, uint32_t* s_touch,
+                                                        const unsigned char* smem, Release release) {
+  const int nsp = NSC >= 0 ? NSC : ns;
+  const bool two_ops = P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL;
+  RegLoader<R> rl;
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= nsp) break;
+    gl.load(q, P.p_col[sparse_probe<true>(P, p0, q)], rl.val[q]);
+  }
+  gl.load(kAggSlot, P.a_col[0], rl.val[kAggSlot]);
+  if (two_ops) gl.load(kAggSlot + 1, P.a_col[1], rl.val[kAggSlot + 1]);
+  release();
+  if (nsp < 2) {
+    sparse_rows<NSC, true>(P, rl, sel, p0, ns, bias, A, s_sum, s_touch, smem);
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  int gv0[MB_MAX_PROBES][R];
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q)
+#pragma unroll
+    for (int i = 0; i < R; ++i) gv0[q][i] = 0;
+  probe_round<R, true>(P, rl, sel, p0, nsp, 0, 1, gv0, A, smem);
+  uint32_t b[R];
+  int c[R], total = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    b[i] = __ballot_sync(kFull, (sel >> i) & 1u);
+    c[i] = __popc(b[i]);
+    total += c[i];
+  }
+  for (int base = 0; base < total; base += 32) {
+    RegLoader<1> r1;
+#pragma unroll
+    for (int j = 0; j < kLoadSlots; ++j) r1.val[j][0] = 0;
+    int g = 0, rem = base + lane;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const bool mine = rem >= 0 && rem < c[i];
+      const int src = mine ? nth_set_lane(b[i], rem) : lane;
+      const int xg = __shfl_sync(kFull, gv0[0][i], src);
+      if (mine) g = xg;
+#pragma unroll
+      for (int j = 1; j < kLoadSlots; ++j) {
+        if (j < MB_MAX_PROBES && j >= nsp) continue;
+        if (j == kAggSlot + 1 && !two_ops) continue;
+        const int x = __shfl_sync(kFull, rl.val[j][i], src);
+        if (mine) r1.val[j][0] = x;
+      }
+      rem -= c[i];
+    }
+    uint32_t s1 = base + lane < total ? 1u : 0u;
+    int gv[MB_MAX_PROBES][1];
+#pragma unroll
+    for (int q = 0; q < MB_MAX_PROBES; ++q) gv[q][0] = 0;
+    gv[0][0] = g;
+    probe_round<1, true>(P, r1, s1, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
+    if (P.count_after < 0) A.cnt += s1;
+    if (s1) aggregate_rows<NSC, 1, true>(P, r1, s1, gv, p0, ns, bias, A, s_sum, s_touch);
+  }
+}
+
 // The sparse phase with cluster-resident mirrors: a probe with a mirror tests presence —
 // and, with payload codes, reads the payload — in the cluster's distributed shared memory
 // instead of L2; probes without one read their tables as in sparse_rows. Payloads a mirror
@@ -451,7 +544,7 @@ __device__ __forceinline__ void sparse_rows_mir(const StarPlan& P, const L& ld, 
       if (q >= nsp) break;
       if (q < qlo || q >= qhi) continue;
       const int p = p0 + q;
-      ld.load(P.p_col[p], v);
+      ld.load(q, P.p_col[p], v);
       const int slots = P.p_slots[p], kmin = P.p_kmin[p], layout = P.p_layout[p], kind = P.mir_kind[p];
       const int base = P.mir_base[p];
       const int* ht = P.p_ht[p];
@@ -515,7 +608,7 @@ __device__ __forceinline__ void sparse_rows_mir(const StarPlan& P, const L& ld, 
     if (q >= nsp) break;
     if (!(fetch[q] & sel)) continue;
     const int p = p0 + q;
-    ld.load(P.p_col[p], v);
+    ld.load(q, P.p_col[p], v);
     const int* ht = P.p_ht[p];
     const bool hi = P.p_layout[p] == MB_HT_KEY_VAL;
 #pragma unroll
@@ -623,7 +716,7 @@ __device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& 
   for (int f = 0; f < P.nf; ++f) {
     if (P.count_after == f) A.cnt += sel;
     if (!sel) continue;
-    ld.load(P.f_col[f], v);
+    ld.load(-1, P.f_col[f], v);
     if (!pass_filter(v[0], P.f_mode[f], P.f_c1[f], P.f_c2[f])) sel = 0;
   }
   if (P.count_after >= P.nf) A.cnt += sel;
@@ -631,17 +724,18 @@ __device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& 
   sparse_rows<-1, false>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
 }
 
-template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false, bool PACK = false>
+template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false, bool PACK = false, bool REL = false>
 __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_constant__ StarPlan P) {
   constexpr int WROWS = 32 * ITEMS;
-  constexpr int TILE = NCW * WROWS;
+  constexpr int NSL = tile_slices(NCW);
+  constexpr int TILE = NSL * WROWS;
   constexpr int NWARPS = NCW + 1;
   constexpr int R = ITEMS / 4 < 2 ? 2 : ITEMS / 4;  // survivors per lane per sparse round
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ unsigned long long s_red[2 * NWARPS];
 
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + kMaxStages;
+  uint64_t* empty = full + 2 * kMaxStages;
   unsigned long long* s_sum = reinterpret_cast<unsigned long long*>(smem + P.smem_groups_off);
   uint32_t* s_touch = reinterpret_cast<uint32_t*>(smem + P.smem_groups_off + 8 * P.total_val);
   int* stage_base = reinterpret_cast<int*>(smem + P.smem_stage_off);
@@ -710,7 +804,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], NCW);
+      mbar_init(&full[S + s], 1);
+      mbar_init(&empty[s], NSL);
     }
     mbar_fence_init();
   }
@@ -733,9 +828,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
       const long long r0 = (b + kk * G) * static_cast<long long>(TILE);
       int* dst = stage_base + ss * stage_words;
       fence_proxy_async_smem();
-      mbar_arrive_expect_tx(&full[ss], stage_words * 4u);
+      uint64_t* fb = &full[kk % (2 * S)];
+      mbar_arrive_expect_tx(fb, stage_words * 4u);
       if (P.gpu_cache == nullptr) {
-        for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, &full[ss], policy);
+        for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, fb, policy);
       } else {
         const long long vseg = r0 >> P.seg_shift;
         const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg])
@@ -743,7 +839,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
         const long long in_seg = r0 & ((1ll << P.seg_shift) - 1);
         for (int c = 0; c < P.ncols; ++c) {
           const long long slot = P.col[c][seg];
-          bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, &full[ss], policy);
+          bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, fb, policy);
         }
       }
     };
@@ -775,7 +871,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
       }
       // no copy may land after the CTA is gone: wait (bounded) for the last ones issued
       for (long long j = (k > S ? k - S : 0); j < k; ++j)
-        if (!mbar_wait_bounded(&full[j % S], static_cast<uint32_t>((j / S) & 1))) failed = true;
+        if (!mbar_wait_bounded(&full[j % (2 * S)], static_cast<uint32_t>((j / (2 * S)) & 1))) failed = true;
     }
   } else {
     // ---- consumers ---------------------------------------------------------------------
@@ -790,17 +886,28 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
       __syncwarp();
       cluster_sync_all();
     }
-    int s = 0;
-    uint32_t phase = 0;
-    for (long long k = 0; k < my_tiles; ++k) {
-      const bool ok = mbar_wait_bounded(&full[s], phase);
+    // Slice j of this CTA's sequence is slice j % NSL of tile j / NSL; warp cw takes
+    // slices cw, cw + NCW, ... (with NCW == NSL: slice cw of every tile). Tile k lands on
+    // full barrier k % 2S, two per stage: a warp that skipped tiles can wait for tile k
+    // while tile k - S, on the same stage, is still landing, and a barrier shared by the
+    // two would show tile k - S's phase. The previous use of barrier k % 2S is tile
+    // k - 2S, which was consumed — so landed — before tile k - S was issued, and tile
+    // k - S was issued before the tile of this warp's previous slice (at most two tiles
+    // back, NCW <= 2 NSL; S >= 2), so the parity wait below is exact.
+    static_assert(NCW <= 2 * NSL, "a warp's consecutive slices must be less than two tiles apart");
+    const long long my_slices = my_tiles * NSL;
+    for (long long j = cw; j < my_slices; j += NCW) {
+      const long long k = j / NSL;
+      const int s = static_cast<int>(k % S);
+      const bool ok = mbar_wait_bounded(&full[k % (2 * S)], static_cast<uint32_t>((k / (2 * S)) & 1));
       if (!__all_sync(kFull, ok)) {
         failed = true;
         break;
       }
-      const int* wstage = stage_base + s * stage_words + cw * WROWS;
+      const int* wstage = stage_base + s * stage_words + static_cast<int>(j % NSL) * WROWS;
       const uint32_t sel = dense_phase<NFC, NDC, ITEMS, TILE>(P, wstage, smem, A);
       const int total = compact(sel, list);
+      bool released = false;
       for (int base = 0; base < total; base += 32 * R) {
         GatherLoader<TILE, R> ld;
         ld.wstage = wstage;
@@ -811,18 +918,25 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
           ld.r[i] = idx < total ? list[idx] : 0;
           if (idx < total) live |= 1u << i;
         }
-        if (MIR)
+        if (REL && base + 32 * R >= total) {
+          // the tile's last batch: its columns go to registers and the stage goes back
+          uint64_t* bar = &empty[s];
+          sparse_rows_packed_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, [bar, lane] {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar);
+          });
+          released = true;
+        } else if (MIR) {
           sparse_rows_mir<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
-        else if (PACK)
+        } else if (PACK) {
           sparse_rows_packed<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
-        else
+        } else {
           sparse_rows<NSC, true>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);
+        }
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
-      if (++s == S) {
-        s = 0;
-        phase ^= 1u;
+      if (!released) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
       }
     }
     // ---- remainder rows (fewer than one tile per CTA), plain loads -----------------
@@ -879,5 +993,6 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
 // Variant tables, one per translation unit that instantiates kernels.
 const Variant* star_variants_generic(int* count);
 const Variant* star_variants_special(int* count);
+const Variant* star_variants_wide(int* count);
 
 }  // namespace mb

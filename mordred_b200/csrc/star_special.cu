@@ -16,6 +16,11 @@ namespace mb {
       {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS, false, true>, false, true},                \
       {8, 16, NF, ND, NS, star_kernel<8, 16, NF, ND, NS, false, true>, false, true}
 
+// the packed shapes that return each stage to the producer before the last batch's probes
+#define MB_REL_VARIANTS(NF, ND, NS)                                                                   \
+  {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS, false, true, true>, false, true, true},            \
+      {16, 8, NF, ND, NS, star_kernel<16, 8, NF, ND, NS, false, true, true>, false, true, true}
+
 // the same shapes reading cluster-resident mirrors in the sparse phase
 #define MB_MIRROR_VARIANTS(NF, ND, NS)                                                        \
   {8, 8, NF, ND, NS, star_kernel<8, 8, NF, ND, NS, true>, true},                              \
@@ -32,6 +37,9 @@ static const Variant kSpecial[] = {
     MB_PACK_VARIANTS(0, 1, 3),
     MB_PACK_VARIANTS(2, 1, 4),
     MB_PACK_VARIANTS(0, 1, 4),
+    MB_REL_VARIANTS(0, 1, 3),
+    MB_REL_VARIANTS(2, 1, 4),
+    MB_REL_VARIANTS(0, 1, 4),
     MB_MIRROR_VARIANTS(0, 1, 2),
     MB_MIRROR_VARIANTS(0, 1, 3),
     MB_MIRROR_VARIANTS(2, 1, 4),

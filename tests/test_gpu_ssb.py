@@ -228,11 +228,11 @@ def test_launch_variants_identical():
     t = ssb.gen_device(s, 17, ssb.QB_FACT, ssb.QB_DIMS)
     ws = ssb.StarWorkspace(s)
     base = ssb.query_b(t, ws).cpu().numpy().copy()
-    for threads in (128, 256, 512):
+    for threads in (128, 256, 512, 640, 768):
         for ipt in (4, 8, 16):
             for stages in (2, 3, 6):
-                if threads == 512 and ipt == 16:
-                    continue
+                if (threads == 512 and ipt == 16) or (threads > 512 and ipt != 8):
+                    continue  # 20 and 24 consumer warps: 8 rows a thread only
                 res = torch.zeros(4 * ssb.QB_GROUPS, dtype=torch.int32, device="cuda")
                 ssb.star_query(_qb_args(t, ws, s, res, threads=threads, items_per_thread=ipt, stages=stages))
                 assert np.array_equal(res.cpu().numpy(), base), (threads, ipt, stages)

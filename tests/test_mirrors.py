@@ -151,23 +151,28 @@ def test_engine_four_table_shape_with_mirrors(cache):
     exp = np.zeros(6 * 175, np.int32)
     assert O.star(n, probes=probes(h, 0), aggr=[h["lo_revenue"], h["lo_supplycost"]], agg_op=1, total_val=175,
                   res_layout=1, res=exp) == 0
-    for mirrors in (2, 1):
+    for mirrors, threads, pack in ((2, 256, 0), (1, 256, 0), (1, 512, 3), (1, 768, 2), (1, 640, 3)):
         got = _run(probes(cols, 1), cols, n, [cols["lo_revenue"], cols["lo_supplycost"]], L.MB_AGG_SUB, 175,
-                   L.MB_RES_ENGINE6, mirrors, 256, 8, **extra)
-        assert np.array_equal(got, exp), (mirrors, cache)
+                   L.MB_RES_ENGINE6, mirrors, threads, 8, pack=pack, **extra)
+        assert np.array_equal(got, exp), (mirrors, threads, pack, cache)
     assert L.device_status(0, clear=True) == 0
 
 
-@pytest.mark.parametrize("threads,items", [(256, 8), (512, 8), (256, 16)])
+@pytest.mark.parametrize("threads,items", [(256, 8), (512, 8), (256, 16), (640, 8), (768, 8)])
 def test_packed_second_round_query_b_and_engine_shapes(threads, items):
-    """The packed second sparse round (mb_star_args.pack = 2) and the plain one (1) equal
-    the oracle for the Query B shape (customer first) and the engine shape (supplier
-    settled by its bitmap and read for its payload after the customer probe)."""
+    """The packed second sparse round (mb_star_args.pack = 2), the packed round that hands
+    each stage back before its last batch of survivors is probed from registers (3) and
+    the plain one (1) equal the oracle for the Query B shape (customer first), the same
+    shape with every supplier present (several survivor batches per warp and tile) and
+    the engine shape (supplier settled by its bitmap and read for its payload after the
+    customer probe). 640 and 768 threads run 20 and 24 consumer warps over tiles of 16
+    slices, handed out round robin."""
     n = 5_000_017
     s, t, h = _tables(n, 91, s_len=20_000, c_len=300_000, p_len=500_000)
     ht = {}
     for name, flt, mode, c1, c2, key, val, slots, kmin, lay in [
             ("s", "s_region", 0, 1, 0, "s_suppkey", None, s.s_len, 0, 0),
+            ("s_all", None, 0, 0, 0, "s_suppkey", None, s.s_len, 0, 0),
             ("c", "c_region", 0, 1, 0, "c_custkey", "c_nation", s.c_len, 0, 1),
             ("p", "p_mfgr", 2, 0, 1, "p_partkey", None, s.p_len, 0, 0),
             ("d", None, 0, 0, 0, "d_datekey", "d_year", ssb.DATE_SLOTS, ssb.DATE_MIN, 1),
@@ -178,7 +183,7 @@ def test_packed_second_round_query_b_and_engine_shapes(threads, items):
         a = np.zeros(2 * slots if lay else slots, np.int32)
         O.build_ht(h[flt] if flt else None, mode, c1, c2, h[key], h[val] if val else None, a, slots, kmin, lay)
         ht[name] = (a, _dev(a))
-    qb = lambda d, k: [dict(fkey=d["lo_suppkey"], ht=ht["s"][k], num_slots=s.s_len, layout=0),
+    qb = lambda d, k, sup="s": [dict(fkey=d["lo_suppkey"], ht=ht[sup][k], num_slots=s.s_len, layout=0),
                        dict(fkey=d["lo_custkey"], ht=ht["c"][k], num_slots=s.c_len, layout=1, unique_val=7,
                             res_slot=1),
                        dict(fkey=d["lo_partkey"], ht=ht["p"][k], num_slots=s.p_len, layout=0),
@@ -191,11 +196,12 @@ def test_packed_second_round_query_b_and_engine_shapes(threads, items):
                         dict(fkey=d["lo_partkey"], ht=ht["p2"][k], num_slots=s.p_len, layout=2),
                         dict(fkey=d["lo_orderdate"], ht=ht["d2"][k], num_slots=ssb.DATE_SLOTS, key_min=ssb.DATE_MIN,
                              layout=2, min_val=1992, unique_val=1, res_slot=3)]
-    for probes, layout, total in ((qb, 2, 175), (eng, 1, 25 * 175)):
+    qb_all = lambda d, k: qb(d, k, "s_all")
+    for probes, layout, total in ((qb, 2, 175), (qb_all, 2, 175), (eng, 1, 25 * 175)):
         exp = np.zeros((4 if layout == 2 else 6) * total, np.int32)
         assert O.star(n, probes=probes(h, 0), aggr=[h["lo_revenue"], h["lo_supplycost"]], agg_op=1, total_val=total,
                       res_layout=layout, res=exp) == 0
-        for pack in (1, 2):
+        for pack in ((1, 2, 3) if threads <= 512 else (2, 3)):
             got = _run(probes(t, 1), t, n, [t["lo_revenue"], t["lo_supplycost"]], L.MB_AGG_SUB, total, layout, 1,
                        threads, items, pack=pack)
             assert np.array_equal(got, exp), (layout, pack, threads, items)
