@@ -126,7 +126,9 @@ typedef struct mb_star_args {
   int64_t start_offset;
   int segment_size;           /* power of two (reference: 1,048,576) */
   /* launch configuration; 0 = the tuned default for this shape */
-  int threads;                /* consumer threads per CTA: 128, 256 or 512 (plus one producer warp) */
+  int threads;                /* consumer threads per CTA: 128, 256 or 512 (plus one producer warp);
+                               * 640 or 768 (20 or 24 warps sharing 16 tile slices, 8 rows a
+                               * thread) where the query shape has such a variant, else 512 */
   int items_per_thread;       /* fact rows per consumer thread per tile: 4, 8 or 16 */
   int stages;                 /* 2..8 bulk-copy stages */
   int grid;                   /* CTAs; 0 = one wave of resident CTAs */

@@ -34,7 +34,7 @@ static const Variant* find_variant(int warps, int items, int nf, int nd, int ns,
         return &sp[i];
   }
   if (mir) return nullptr;
-  if (rel) return find_variant(warps, items, nf, nd, ns, false, true, false);  // no early-release variant
+  if (rel) return find_variant(warps, items, nf, nd, ns, false, true, false);  // no early-return variant
   if (pack) return find_variant(warps, items, nf, nd, ns, false, false);  // no packing variant: plain one
   const Variant* g = star_variants_generic(&n);
   for (int i = 0; i < n; ++i)
@@ -325,6 +325,15 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   if (smem > budget) return MB_ERR_SIZE;
   if (var == nullptr)
     var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, want_pack, want_rel);
+  if (var == nullptr && ncw > kMaxTileSlices) {
+    // wide launches (more consumer warps than tile slices) are compiled for the packed
+    // shapes only; a call whose plan lands on another shape — small dimension tables
+    // that get a staged bitmap and join the dense phase, or misaligned columns that
+    // leave only the per-row path — takes 16 consumer warps
+    mb_star_args narrow = *a;
+    narrow.threads = kMaxTileSlices * 32;
+    return launch_star(&narrow, stream, count32, preset);
+  }
   if (var == nullptr) return MB_ERR_ARG;
 
   // sparse visiting order of the tiled path: chain order, except that the first probe

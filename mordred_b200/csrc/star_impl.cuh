@@ -824,11 +824,13 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     long long k = 0;
     int s = 0;
     uint32_t phase = 0;  // use count of stage s, mod 2
-    auto issue = [&](long long kk, int ss) {
+    // tile kk goes to stage ss = kk % S and lands on full barrier kk % 2S = ss + S * (use
+    // count of the stage mod 2)
+    auto issue = [&](long long kk, int ss, uint32_t use) {
       const long long r0 = (b + kk * G) * static_cast<long long>(TILE);
       int* dst = stage_base + ss * stage_words;
       fence_proxy_async_smem();
-      uint64_t* fb = &full[kk % (2 * S)];
+      uint64_t* fb = &full[ss + S * static_cast<int>(use)];
       mbar_arrive_expect_tx(fb, stage_words * 4u);
       if (P.gpu_cache == nullptr) {
         for (int c = 0; c < P.ncols; ++c) bulk_g2s(dst + c * TILE, P.col[c] + r0, TILE * 4, fb, policy);
@@ -847,7 +849,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
       // fill the ring while the consumers build the mirrors, then join the cluster barrier
       if (lane == 0) {
         for (; k < my_tiles && k < S; ++k) {
-          issue(k, s);
+          issue(k, s, phase);
           if (++s == S) {
             s = 0;
             phase ^= 1u;
@@ -863,7 +865,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
           failed = true;
           break;
         }
-        issue(k, s);
+        issue(k, s, phase);
         if (++s == S) {
           s = 0;
           phase ^= 1u;
@@ -895,16 +897,28 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
     // k - S was issued before the tile of this warp's previous slice (at most two tiles
     // back, NCW <= 2 NSL; S >= 2), so the parity wait below is exact.
     static_assert(NCW <= 2 * NSL, "a warp's consecutive slices must be less than two tiles apart");
-    const long long my_slices = my_tiles * NSL;
-    for (long long j = cw; j < my_slices; j += NCW) {
-      const long long k = j / NSL;
-      const int s = static_cast<int>(k % S);
-      const bool ok = mbar_wait_bounded(&full[k % (2 * S)], static_cast<uint32_t>((k / (2 * S)) & 1));
+    long long k = 0;                   // tile of the current slice
+    int sl = cw, s = 0, fb = 0;        // slice in the tile, stage k % S, full barrier k % 2S
+    uint32_t par = 0;                  // parity of tile k's phase on barrier fb
+    auto next_tile = [&]() {
+      ++k;
+      if (++s == S) s = 0;
+      if (++fb == 2 * S) {
+        fb = 0;
+        par ^= 1u;
+      }
+    };
+    while (sl >= NSL) {
+      sl -= NSL;
+      next_tile();
+    }
+    for (; k < my_tiles;) {
+      const bool ok = mbar_wait_bounded(&full[fb], par);
       if (!__all_sync(kFull, ok)) {
         failed = true;
         break;
       }
-      const int* wstage = stage_base + s * stage_words + static_cast<int>(j % NSL) * WROWS;
+      const int* wstage = stage_base + s * stage_words + sl * WROWS;
       const uint32_t sel = dense_phase<NFC, NDC, ITEMS, TILE>(P, wstage, smem, A);
       const int total = compact(sel, list);
       bool released = false;
@@ -920,6 +934,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
         }
         if (REL && base + 32 * R >= total) {
           // the tile's last batch: its columns go to registers and the stage goes back
+          // before its probes (handing it back after the first probe round, with only the
+          // kept rows copied, measured slower: the stage is held through an L2 round trip)
           uint64_t* bar = &empty[s];
           sparse_rows_packed_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, [bar, lane] {
             __syncwarp();
@@ -937,6 +953,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
       if (!released) {
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
+      }
+      sl += NCW;
+      while (sl >= NSL) {
+        sl -= NSL;
+        next_tile();
       }
     }
     // ---- remainder rows (fewer than one tile per CTA), plain loads -----------------
