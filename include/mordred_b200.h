@@ -149,8 +149,8 @@ typedef struct mb_star_args {
    * kept are moved one a lane before the later probes and the aggregate run): 0 = the
    * tuned default for the shape, 1 = never, 2 = where the shape has a packed variant,
    * 3 = packed, with each tile's stage handed back to the bulk-copy producer before its
-   * last batch of survivors is probed (their columns held in registers). Results are the
-   * same either way. */
+   * last batch of survivors is probed (their columns held in registers), 4 = unpacked,
+   * with that early return. Results are the same either way. */
   int pack;
 } mb_star_args;
 

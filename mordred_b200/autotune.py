@@ -126,10 +126,11 @@ def tune(n: int = 120_000_000, reps: int = 5, verbose: bool = True) -> list[dict
     results = []
     for name, bpr, key, make in shapes:
         runs = []
-        packed = tuple(key) in PACKED_SHAPES
-        threads = THREADS + (WIDE_THREADS if packed else ())
-        # mb_star_args.pack: 1 plain, 2 packed, 3 packed with early stage return
-        packs = (1, 2, 3) if packed else (1,)
+        packed, early = tuple(key) in PACKED_SHAPES, tuple(key) in EARLY_RETURN_SHAPES
+        threads = THREADS + (WIDE_THREADS if packed or early else ())
+        # mb_star_args.pack: 1 plain, 2 packed, 3 packed with early stage return, 4 unpacked
+        # with early stage return
+        packs = (1, 2, 3) if packed else (1, 4) if early else (1,)
         for th, it, stg, gm, pk in itertools.product(threads, ITEMS, STAGES, (1, 2), packs):
             if key[3] == 0 and gm == 2:
                 continue  # scalar results have no group array
@@ -210,6 +211,9 @@ def tune_small(n: int = 6_000_000, copies: int = 20, reps: int = 10, verbose: bo
 # the kept rows copied, measured 0.638 / 0.674 ms against 0.611 / 0.653 ms. The tuned
 # entry's pack field: 1 packed, 2 packed with early stage return.
 PACKED_SHAPES = {(0, 4, 0, 1, 0), (0, 4, 2, 1, 0)}
+# Shapes with unpacked early-return variants (20 or 24 consumer warps): Query A, 0.4526
+# against 0.460 ms for three 8-warp CTAs a SM (it already had 24 consumer warps a SM).
+EARLY_RETURN_SHAPES = {(0, 3, 0, 1, 1)}
 
 
 def write(results: list[dict], gpu: str) -> None:

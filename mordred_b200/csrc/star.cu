@@ -34,7 +34,7 @@ static const Variant* find_variant(int warps, int items, int nf, int nd, int ns,
         return &sp[i];
   }
   if (mir) return nullptr;
-  if (rel) return find_variant(warps, items, nf, nd, ns, false, true, false);  // no early-return variant
+  if (rel) return find_variant(warps, items, nf, nd, ns, false, pack, false);  // no early-return variant
   if (pack) return find_variant(warps, items, nf, nd, ns, false, false);  // no packing variant: plain one
   const Variant* g = star_variants_generic(&n);
   for (int i = 0; i < n; ++i)
@@ -287,9 +287,9 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   if (group_mode == 1 && P.gmode != kGroupSmem) return MB_ERR_SIZE;
 
   if (a->mirrors < 0 || a->mirrors > 2) return MB_ERR_ARG;
-  if (a->pack < 0 || a->pack > 3) return MB_ERR_ARG;
-  const bool want_pack = a->pack >= 2 || (a->pack == 0 && tc.pack != 0);
-  const bool want_rel = a->pack == 3 || (a->pack == 0 && tc.pack == 2);
+  if (a->pack < 0 || a->pack > 4) return MB_ERR_ARG;
+  const bool want_pack = a->pack == 2 || a->pack == 3 || (a->pack == 0 && (tc.pack == 1 || tc.pack == 2));
+  const bool want_rel = a->pack >= 3 || (a->pack == 0 && tc.pack >= 2);
   const int budget = ds->max_smem_optin - 2048 - 2 * 8 * (ncw + 1);
   const int want_stages = a->stages ? a->stages : tc.stages;
   if (want_stages < 2 || want_stages > kMaxStages) return MB_ERR_ARG;

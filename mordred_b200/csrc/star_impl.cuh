@@ -24,7 +24,7 @@ struct Variant {
   KernelFn fn;
   bool mir = false;   // reads cluster-resident mirrors (launched with a cluster)
   bool pack = false;  // packs the first sparse probe's survivors across the warp
-  bool rel = false;   // packed, and returns each stage before its last batch's probes
+  bool rel = false;   // returns each stage before its last batch's probes (columns in registers)
 };
 
 __device__ __forceinline__ bool pass_filter(int x, int mode, int c1, int c2) {
@@ -433,6 +433,34 @@ __device__ __forceinline__ void sparse_rows_packed(const StarPlan& P, const Gath
   }
 }
 
+// The columns the sparse phase reads for a batch (every sparse probe key, the aggregate
+// operands), copied from the stage into registers.
+template <int NSC, int TILE, int R>
+__device__ __forceinline__ void copy_to_regs(const StarPlan& P, const GatherLoader<TILE, R>& gl, int p0, int ns,
+                                             RegLoader<R>& rl) {
+  const int nsp = NSC >= 0 ? NSC : ns;
+#pragma unroll
+  for (int q = 0; q < MB_MAX_PROBES; ++q) {
+    if (q >= nsp) break;
+    gl.load(q, P.p_col[sparse_probe<true>(P, p0, q)], rl.val[q]);
+  }
+  gl.load(kAggSlot, P.a_col[0], rl.val[kAggSlot]);
+  if (P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL) gl.load(kAggSlot + 1, P.a_col[1], rl.val[kAggSlot + 1]);
+}
+
+// sparse_rows for a warp's last batch of a tile, returning the stage early: the batch's
+// columns go to registers, `release()` hands the stage back, and both probe rounds run
+// from registers. Warp-converged.
+template <int NSC, int TILE, int R, class Release>
+__device__ __forceinline__ void sparse_rows_regs(const StarPlan& P, const GatherLoader<TILE, R>& gl, uint32_t sel,
+                                                 int p0, int ns, unsigned bias, Accum& A, unsigned long long* s_sum,
+                                                 uint32_t* s_touch, const unsigned char* smem, Release release) {
+  RegLoader<R> rl;
+  copy_to_regs<NSC>(P, gl, p0, ns, rl);
+  release();
+  sparse_rows<NSC, true>(P, rl, sel, p0, ns, bias, A, s_sum, s_touch, smem);
+}
+
 // sparse_rows_packed for a warp's last batch of a tile, returning the stage early: the
 // survivors' columns that the sparse phase reads (every sparse probe key and the
 // aggregate operands) are copied into registers, `release()` hands the stage back to
@@ -448,13 +476,7 @@ __device__ __forceinline__ void sparse_rows_packed_regs(const StarPlan& P, const
   const int nsp = NSC >= 0 ? NSC : ns;
   const bool two_ops = P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL;
   RegLoader<R> rl;
-#pragma unroll
-  for (int q = 0; q < MB_MAX_PROBES; ++q) {
-    if (q >= nsp) break;
-    gl.load(q, P.p_col[sparse_probe<true>(P, p0, q)], rl.val[q]);
-  }
-  gl.load(kAggSlot, P.a_col[0], rl.val[kAggSlot]);
-  if (two_ops) gl.load(kAggSlot + 1, P.a_col[1], rl.val[kAggSlot + 1]);
+  copy_to_regs<NSC>(P, gl, p0, ns, rl);
   release();
   if (nsp < 2) {
     sparse_rows<NSC, true>(P, rl, sel, p0, ns, bias, A, s_sum, s_touch, smem);
@@ -937,10 +959,14 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_co
           // before its probes (handing it back after the first probe round, with only the
           // kept rows copied, measured slower: the stage is held through an L2 round trip)
           uint64_t* bar = &empty[s];
-          sparse_rows_packed_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, [bar, lane] {
+          auto give_back = [bar, lane] {
             __syncwarp();
             if (lane == 0) mbar_arrive(bar);
-          });
+          };
+          if (PACK)
+            sparse_rows_packed_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, give_back);
+          else
+            sparse_rows_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, give_back);
           released = true;
         } else if (MIR) {
           sparse_rows_mir<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem);

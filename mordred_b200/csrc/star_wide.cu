@@ -12,7 +12,13 @@ namespace mb {
       {20, 8, NF, ND, NS, star_kernel<20, 8, NF, ND, NS, false, true, true>, false, true, true},         \
       {24, 8, NF, ND, NS, star_kernel<24, 8, NF, ND, NS, false, true, true>, false, true, true}
 
+// unpacked, returning each stage early (the Query A shape: its second round is one small table)
+#define MB_WIDE_PLAIN_VARIANTS(NF, ND, NS)                                                               \
+  {20, 8, NF, ND, NS, star_kernel<20, 8, NF, ND, NS, false, false, true>, false, false, true},           \
+      {24, 8, NF, ND, NS, star_kernel<24, 8, NF, ND, NS, false, false, true>, false, false, true}
+
 static const Variant kWide[] = {
+    MB_WIDE_PLAIN_VARIANTS(0, 1, 2),  // Query A
     MB_WIDE_VARIANTS(0, 1, 3),  // Query B
     MB_WIDE_VARIANTS(2, 1, 4),  // engine filter_probe_group_by
     MB_WIDE_VARIANTS(0, 1, 4),  // engine probe_group_by

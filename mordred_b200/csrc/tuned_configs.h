@@ -14,7 +14,8 @@ struct TunedConfig {
   int threads, items, stages, group_mode;
   int mirrors = 0;  // 1: large calls of this shape use cluster-resident mirrors by default
   int pack = 0;     // 1: the variant that packs the first sparse probe's survivors across the warp;
-                    // 2: packed, returning each stage before its last batch's probes
+                    // 2: packed, returning each stage before its last batch's probes; 3: unpacked,
+                    // with that early return
 };
 
 struct TunedEntry {
@@ -28,7 +29,7 @@ static const TunedConfig kDefaultConfig = {256, 8, 2, 0};
 static const TunedEntry kTuned[] = {
     {3, 0, -1, 0, 0, {128, 16, 3, 0}, 16ll << 20},  // filter-aggregate, 6 M rows: 0.0185 ms, 5.19 TB/s
     {3, 0, -1, 0, 0, {256, 16, 4, 0}},  // filter-aggregate (q11 form): 0.268 ms, 7.16 TB/s
-    {0, 3, 0, 1, 1, {256, 8, 2, 2}},  // Query A form: 0.452 ms, 4.25 TB/s
+    {0, 3, 0, 1, 1, {768, 8, 3, 2, 0, 3}},  // Query A form: 0.453 ms, 4.24 TB/s (24 warps, early stage return)
     {0, 4, 0, 1, 0, {768, 8, 2, 1, 0, 2}},  // Query B form: 0.627 ms, 4.59 TB/s (24 warps, packed, early stage return)
     {0, 4, 2, 1, 0, {768, 8, 2, 1, 0, 2}},  // engine four-table group-by: 0.666 ms, 4.32 TB/s (customer first, 24 warps, packed, early return)
 };

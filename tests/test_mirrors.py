@@ -105,6 +105,11 @@ def test_query_a_shape_with_mirrors(threads, items):
         got = _run(probes(t, 1), t, n, [t["lo_revenue"]], L.MB_AGG_SUM, ssb.QA_GROUPS, L.MB_RES_CRYSTAL4, mirrors,
                    threads, items)
         assert np.array_equal(got, exp), (mirrors, threads, items)
+    # unpacked early stage return, 16 / 20 / 24 consumer warps, shared-memory and L2 groups
+    for wide, group_mode in ((threads, 0), (640, 1), (768, 2), (768, 1)):
+        got = _run(probes(t, 1), t, n, [t["lo_revenue"]], L.MB_AGG_SUM, ssb.QA_GROUPS, L.MB_RES_CRYSTAL4, 1,
+                   wide, 8, pack=4, group_mode=group_mode)
+        assert np.array_equal(got, exp), (wide, group_mode)
     assert L.device_status(0, clear=True) == 0
 
 
