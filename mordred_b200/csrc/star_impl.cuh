@@ -746,8 +746,14 @@ __device__ __forceinline__ void tail_row(const StarPlan& P, const L& ld, Accum& 
   sparse_rows<-1, false>(P, ld, sel, 0, P.np, static_cast<unsigned>(P.group_bias), A, s_sum, s_touch, smem);
 }
 
+// CTAs per SM the register budget must allow for a variant of NCW consumer warps: the
+// small-CTA shapes run two (8 warps) or four (4 warps) CTAs an SM where their stages fit,
+// and a register or two more per thread would cost a whole CTA (each scheduler's 16 K
+// registers are split among its warps).
+constexpr int star_min_ctas(int ncw) { return ncw <= 4 ? 4 : ncw <= 8 ? 2 : 1; }
+
 template <int NCW, int ITEMS, int NFC, int NDC, int NSC, bool MIR = false, bool PACK = false, bool REL = false>
-__global__ void __launch_bounds__((NCW + 1) * 32, 1) star_kernel(const __grid_constant__ StarPlan P) {
+__global__ void __launch_bounds__((NCW + 1) * 32, star_min_ctas(NCW)) star_kernel(const __grid_constant__ StarPlan P) {
   constexpr int WROWS = 32 * ITEMS;
   constexpr int NSL = tile_slices(NCW);
   constexpr int TILE = NSL * WROWS;
