@@ -382,9 +382,16 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) batch_kernel(const __grid_c
             const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg]) : static_cast<int>(vseg);
             const long long in = r & (S - 1);
             const int take = static_cast<int>(S - in < TILE - done ? S - in : TILE - done);
-            for (int c = 0; c < P.ncols; ++c)
-              bulk_g2s(dst + c * CS + done, P.gpu_cache + (static_cast<long long>(P.col[c][seg]) << P.seg_shift) + in,
-                       static_cast<uint32_t>(take) * 4u, &full[s], policy);
+            // all slots first (their loads in flight together), then the ordered copies
+            int slot[MB_NUM_FACT_COLS];
+#pragma unroll
+            for (int c = 0; c < MB_NUM_FACT_COLS; ++c)
+              if (c < P.ncols) slot[c] = P.col[c][seg];
+#pragma unroll
+            for (int c = 0; c < MB_NUM_FACT_COLS; ++c)
+              if (c < P.ncols)
+                bulk_g2s(dst + c * CS + done, P.gpu_cache + (static_cast<long long>(slot[c]) << P.seg_shift) + in,
+                         static_cast<uint32_t>(take) * 4u, &full[s], policy);
             done += take;
           }
         }

@@ -867,10 +867,18 @@ __global__ void __launch_bounds__((NCW + 1) * 32, star_min_ctas(NCW)) star_kerne
         const int seg = P.seg_group ? static_cast<int>(P.seg_group[vseg])
                                     : static_cast<int>((P.start_offset + r0) >> P.seg_shift);
         const long long in_seg = r0 & ((1ll << P.seg_shift) - 1);
-        for (int c = 0; c < P.ncols; ++c) {
-          const long long slot = P.col[c][seg];
-          bulk_g2s(dst + c * TILE, P.gpu_cache + (slot << P.seg_shift) + in_seg, TILE * 4, fb, policy);
-        }
+        // every column's cache slot first (independent loads in flight together), then
+        // the copies: a copy is an ordered asm statement, so a slot load placed between
+        // two copies would wait for the previous load to return
+        int slot[kMaxCols];
+#pragma unroll
+        for (int c = 0; c < kMaxCols; ++c)
+          if (c < P.ncols) slot[c] = P.col[c][seg];
+#pragma unroll
+        for (int c = 0; c < kMaxCols; ++c)
+          if (c < P.ncols)
+            bulk_g2s(dst + c * TILE, P.gpu_cache + (static_cast<long long>(slot[c]) << P.seg_shift) + in_seg,
+                     TILE * 4, fb, policy);
       }
     };
     if (MIR) {
