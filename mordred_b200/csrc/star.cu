@@ -66,7 +66,7 @@ static int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
 // Lay out shared memory for `stages` stages; returns total bytes. A mirror share (P.cluster >
 // 1) sits between the survivor lists and the stage ring.
-static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_bitmaps) {
+static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_bitmaps, bool xfer) {
   const int tile = tile_slices(ncw) * 32 * items;
   int off = 3 * kMaxStages * 8;  // full (two per stage) and empty mbarriers
   P.smem_groups_off = off;
@@ -113,7 +113,7 @@ static int layout_smem(StarPlan& P, int ncw, int items, int stages, bool stage_b
   }
   off = round_up(off, 16);
   P.smem_list_off = off;
-  off += ncw * 32 * items * 2;
+  off += ncw * star_list_bytes(items, xfer);
   off = round_up(off, 16);
   P.smem_mirror_off = off;
   if (P.cluster > 1) off += 4 << P.mir_shift;
@@ -294,13 +294,14 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
   const int want_stages = a->stages ? a->stages : tc.stages;
   if (want_stages < 2 || want_stages > kMaxStages) return MB_ERR_ARG;
   clear_mirrors(P);
+  const bool xfer = want_pack && want_rel;  // the survivor lists double as the packing buffer
   auto fit = [&]() -> int {
-    int smem = layout_smem(P, ncw, items, want_stages, true);
-    while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);
+    int smem = layout_smem(P, ncw, items, want_stages, true, xfer);
+    while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true, xfer);
     if (smem > budget && P.gmode == kGroupSmem && group_mode != 1) {
       P.gmode = kGroupGlobal;
-      smem = layout_smem(P, ncw, items, want_stages, true);
-      while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true);
+      smem = layout_smem(P, ncw, items, want_stages, true, xfer);
+      while (smem > budget && P.stages > 2) smem = layout_smem(P, ncw, items, P.stages - 1, true, xfer);
     }
     return smem;
   };
@@ -321,7 +322,7 @@ int launch_star(const mb_star_args* a, cudaStream_t stream, int count32, const D
       smem = fit();
     }
   }
-  if (smem > budget) smem = layout_smem(P, ncw, items, 2, false);
+  if (smem > budget) smem = layout_smem(P, ncw, items, 2, false, xfer);
   if (smem > budget) return MB_ERR_SIZE;
   if (var == nullptr)
     var = find_variant(ncw, items, P.nf, P.n_dense, P.np - P.sparse_p0, false, want_pack, want_rel);

@@ -32,6 +32,14 @@ constexpr int kMaxTileSlices = 16;
 __host__ __device__ constexpr int tile_slices(int consumer_warps) {
   return consumer_warps > kMaxTileSlices ? kMaxTileSlices : consumer_warps;
 }
+// Per-warp shared memory for the survivor list (a 16-bit row offset per slice row). The
+// packed variants that return the stage early reuse it after the last batch's gather to
+// hand the first probe's kept rows to their packed lanes: 32 rows of kXferWords ints (an
+// odd stride, so the 32 rows fall in distinct banks).
+constexpr int kXferWords = 7;
+__host__ __device__ constexpr int star_list_bytes(int items, bool xfer) {
+  return xfer && 32 * kXferWords * 4 > 64 * items ? 32 * kXferWords * 4 : 64 * items;
+}
 constexpr int kSmemGroupMax = 8192;            // groups kept in shared memory per CTA
 constexpr int kBitmapSmemMaxBytes = 32768;     // largest presence bitmap staged (262,144 slots)
 constexpr int kBitmapSmemTotalBytes = 40960;

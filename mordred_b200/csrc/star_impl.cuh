@@ -465,14 +465,17 @@ __device__ __forceinline__ void sparse_rows_regs(const StarPlan& P, const Gather
 // survivors' columns that the sparse phase reads (every sparse probe key and the
 // aggregate operands) are copied into registers, `release()` hands the stage back to
 // the producer, and the two probe rounds — with their L2 round trips — run from
-// registers while the next tile lands. After the first probe the kept rows are packed
-// across the warp with all their column values (shuffles), as in sparse_rows_packed.
-// Warp-converged: every lane calls it.
+// registers while the next tile lands. After the first probe each kept row is written,
+// with its payload and its other columns, to its packed position (item-major: every
+// lane's item 0 first) in the warp's buffer `xfer` (the survivor list, read already:
+// 32 rows of kXferWords ints), and each lane reads one packed row back — a scatter, with
+// no search for source lanes. Warp-converged: every lane calls it.
 template <int NSC, int TILE, int R, class Release>
 __device__ __forceinline__ void sparse_rows_packed_regs(const StarPlan& P, const GatherLoader<TILE, R>& gl,
                                                         uint32_t sel, int p0, int ns, unsigned bias, Accum& A,
                                                         unsigned long long* s_sum, uint32_t* s_touch,
-                                                        const unsigned char* smem, Release release) {
+                                                        const unsigned char* smem, int* xfer, Release release) {
+  static_assert(kXferWords >= kLoadSlots, "a packed row holds the payload and every column slot");
   const int nsp = NSC >= 0 ? NSC : ns;
   const bool two_ops = P.agg_op == MB_AGG_SUB || P.agg_op == MB_AGG_MUL;
   RegLoader<R> rl;
@@ -497,31 +500,35 @@ __device__ __forceinline__ void sparse_rows_packed_regs(const StarPlan& P, const
     c[i] = __popc(b[i]);
     total += c[i];
   }
+  const uint32_t below = (1u << lane) - 1u;
+  // slot j of a packed row: 0 the first probe's payload, 1..nsp-1 the later probe keys,
+  // kAggSlot.. the aggregate operands
+  auto used = [&](int j) { return !(j < MB_MAX_PROBES && j >= nsp) && !(j == kAggSlot + 1 && !two_ops); };
   for (int base = 0; base < total; base += 32) {
-    RegLoader<1> r1;
-#pragma unroll
-    for (int j = 0; j < kLoadSlots; ++j) r1.val[j][0] = 0;
-    int g = 0, rem = base + lane;
+    int first = -base;  // packed position of this group's first row of item i
 #pragma unroll
     for (int i = 0; i < R; ++i) {
-      const bool mine = rem >= 0 && rem < c[i];
-      const int src = mine ? nth_set_lane(b[i], rem) : lane;
-      const int xg = __shfl_sync(kFull, gv0[0][i], src);
-      if (mine) g = xg;
+      const int pos = first + __popc(b[i] & below);
+      if (((sel >> i) & 1u) && pos >= 0 && pos < 32) {
+        int* dst = xfer + pos * kXferWords;
+        dst[0] = gv0[0][i];
 #pragma unroll
-      for (int j = 1; j < kLoadSlots; ++j) {
-        if (j < MB_MAX_PROBES && j >= nsp) continue;
-        if (j == kAggSlot + 1 && !two_ops) continue;
-        const int x = __shfl_sync(kFull, rl.val[j][i], src);
-        if (mine) r1.val[j][0] = x;
+        for (int j = 1; j < kLoadSlots; ++j)
+          if (used(j)) dst[j] = rl.val[j][i];
       }
-      rem -= c[i];
+      first += c[i];
     }
-    uint32_t s1 = base + lane < total ? 1u : 0u;
+    __syncwarp();
+    RegLoader<1> r1;
+    const int* src = xfer + lane * kXferWords;
     int gv[MB_MAX_PROBES][1];
 #pragma unroll
     for (int q = 0; q < MB_MAX_PROBES; ++q) gv[q][0] = 0;
-    gv[0][0] = g;
+    gv[0][0] = src[0];
+#pragma unroll
+    for (int j = 1; j < kLoadSlots; ++j) r1.val[j][0] = used(j) ? src[j] : 0;
+    __syncwarp();  // every read done before the next group's writes or the list's next use
+    uint32_t s1 = base + lane < total ? 1u : 0u;
     probe_round<1, true>(P, r1, s1, p0, nsp, 1, MB_MAX_PROBES, gv, A, smem);
     if (P.count_after < 0) A.cnt += s1;
     if (s1) aggregate_rows<NSC, 1, true>(P, r1, s1, gv, p0, ns, bias, A, s_sum, s_touch);
@@ -914,7 +921,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, star_min_ctas(NCW)) star_kerne
   } else {
     // ---- consumers ---------------------------------------------------------------------
     const int cw = warp - 1;
-    uint16_t* list = reinterpret_cast<uint16_t*>(smem + P.smem_list_off) + cw * WROWS;
+    constexpr int LIST_BYTES = star_list_bytes(ITEMS, PACK && REL);
+    uint16_t* list = reinterpret_cast<uint16_t*>(smem + P.smem_list_off + cw * LIST_BYTES);
     const int nd = P.sparse_p0;  // the sparse phase starts at probe sparse_p0 <= n_dense
     const int ns = NSC >= 0 ? NSC : P.np - P.sparse_p0;
     const unsigned sparse_bias = static_cast<unsigned>(P.group_bias) + P.dense_bias;
@@ -978,7 +986,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, star_min_ctas(NCW)) star_kerne
             if (lane == 0) mbar_arrive(bar);
           };
           if (PACK)
-            sparse_rows_packed_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, give_back);
+            sparse_rows_packed_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem,
+                                         reinterpret_cast<int*>(list), give_back);
           else
             sparse_rows_regs<NSC>(P, ld, live, nd, ns, sparse_bias, A, s_sum, s_touch, smem, give_back);
           released = true;
