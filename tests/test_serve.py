@@ -166,6 +166,15 @@ def test_router_prefers_the_gpu_until_it_has_seen_gpu_latencies():
     assert not r.route(0, B.generate_queries(1, seed=1)[0])
 
 
+def test_router_keeps_at_most_max_inflight_queries_on_the_cpu():
+    r = S.PlannerRouter.__new__(S.PlannerRouter)
+    r.gpu_lat = __import__("collections").deque([300.0] * 16, maxlen=64)
+    r.considered = 0
+    r.gpu_target_ms = 100.0
+    r.max_inflight, r.inflight = 1, 1
+    assert not r.route(0, B.generate_queries(1, seed=1)[0])  # busy: never reaches the model
+
+
 def test_router_keeps_queries_on_the_gpu_while_it_meets_its_latency_target():
     r = S.PlannerRouter.__new__(S.PlannerRouter)
     r.gpu_lat = __import__("collections").deque([30.0] * 16, maxlen=64)
@@ -194,7 +203,7 @@ def test_router_sends_queries_to_the_cpu_with_exact_results(server):
         S.CircularServer(t, sizes, n, budget_bytes=4 << 20, max_active=64, chunks=4)
     qs = B.generate_queries(240, seed=12, sel_lo=1e-4, sel_hi=0.3)
     arr = S.poisson_arrivals(1500.0, len(qs), 13)
-    router = S.PlannerRouter(table, _CheapCpu(), margin=1.0, max_backlog_ms=1e9, gpu_target_ms=0.0)
+    router = S.PlannerRouter(table, _CheapCpu(), margin=1.0, max_backlog_ms=1e9, gpu_target_ms=0.0, max_inflight=8)
     rep, res = srv.serve(qs, arr, keep_results=True, router=router)
     router.close()
     s = rep.summary(n)
