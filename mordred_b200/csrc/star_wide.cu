@@ -1,7 +1,8 @@
-// star_wide.cu — kernel variants with more consumer warps than tile slices (20 or 24
-// warps over 16 slices of 256 rows; 28 measured no faster than 24), for the packed shapes whose sparse phase waits on L2:
-// the extra warps probe the survivors of earlier slices while others stream later ones.
-// In a translation unit of their own so the build compiles them in parallel.
+// star_wide.cu — kernel variants with more consumer warps than tile slices: 20 or 24 warps
+// over 16 slices of 256 rows (28 measured no faster than 24). A warp copies its last
+// batch's columns into registers and returns the stage before it probes, so the extra
+// warps probe the survivors of earlier slices while others run the dense phase of later
+// ones. In a translation unit of their own so the build compiles them in parallel.
 #include "star_impl.cuh"
 
 namespace mb {

@@ -31,7 +31,7 @@ static const TunedEntry kTuned[] = {
     {3, 0, -1, 0, 0, {256, 16, 4, 0}},  // filter-aggregate (q11 form): 0.2684 ms, 7.15 TB/s
     {0, 3, 0, 1, 1, {768, 8, 3, 2, 0, 3}},  // Query A form: 0.4558 ms, 4.21 TB/s (24 warps, early stage return)
     {0, 4, 0, 1, 0, {768, 8, 2, 1, 0, 2}},  // Query B form: 0.5942 ms, 4.85 TB/s (24 warps, packed, early stage return)
-    {0, 4, 2, 1, 0, {768, 8, 2, 1, 0, 2}},  // engine four-table group-by: 0.6432 ms, 4.48 TB/s (customer first, 24 warps, packed, early return)
+    {0, 4, 2, 1, 0, {768, 8, 2, 1, 0, 2}},  // engine four-table group-by: 0.6432 ms, 4.48 TB/s (24 warps, packed, early return)
 };
 
 inline TunedConfig tuned_config(int nf, int np, int p0_layout, int res_layout, int total_val, long long rows) {
